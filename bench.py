@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark of the device-wide algorithm path on B200.
+
+Headline workload (one "step"): sum-reduce and inclusive sum-scan over
+N = 2^28 elements of each of float32 U[-1,1], float64 U[-1,1] and int32
+U[-100,100] -- six library calls per step.  The inputs (1 + 2 + 1 GiB) are
+larger than L2, so no flush is needed between steps.
+
+value  = algorithmic bytes per step (reduce N*s, scan 2*N*s) / device time,
+         whole job over all ranks (each rank runs the same workload on its own
+         GPU: replicas, weak scaling).
+e2e    = the same through the C-ABI with host buffers: pinned-host -> device
+         copies of the step's inputs and device -> host copies of every result
+         inside the timed region.
+ops    = per-op GB/s at the other benchmark configurations (merge_by_key,
+         stable sort_by_key, reduce_by_key), timed after the headline.
+
+``--impl reference`` times the reference's CPU implementation of the same
+reduce + scan on the host cores instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "effective GB/s & %HBM peak per op at 2^26-2^28; batched req/s + p99 vs plain"
+WORKLOAD = "reduce+inclusive_scan sum, N=2^28, f32 U[-1,1] + f64 U[-1,1] + i32 U[-100,100]"
+N_HEADLINE = 1 << 28
+DTYPES = [("f32", 4), ("f64", 8), ("i32", 4)]
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return None
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                rows.append((float(c[1]), float(c[2]), c[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------
+def run_reference(args):
+    """CPU reference arm: the reference's reduce + scan structure on all host cores."""
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return 0
+    line = cpu_reference_line(args.steps, args.warmup)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_reference_time(n_sample: int, steps: int, warmup: int, threads: int):
+    """Seconds per sample-step of reduce + scan over n_sample elements of each dtype."""
+    import ctypes
+
+    import numpy as np
+
+    from oracle import _lib as olib  # CPU baseline leg: the oracle's threaded restatement
+    import oracle
+    red = olib.bko_baseline_reduce
+    red.restype = ctypes.c_double
+    red.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+    scn = olib.bko_baseline_inclusive_scan
+    scn.restype = None
+    scn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+    data = [(oracle.gen(np.float32, n_sample, 0, -1.0, 1.0), 0), (oracle.gen(np.float64, n_sample, 0, -1.0, 1.0), 1),
+            (oracle.gen(np.int32, n_sample, 0, -100, 100), 2)]
+    outs = [np.empty_like(x) for x, _ in data]
+
+    def step():
+        for (x, t), o in zip(data, outs):
+            red(x.ctypes.data, x.size, t, threads)
+            scn(x.ctypes.data, o.ctypes.data, x.size, t, threads)
+
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    return (time.perf_counter() - t0) / steps
+
+
+def cpu_reference_line(steps, warmup):
+    threads = os.cpu_count() or 1
+    n_sample = 1 << 24
+    sec = cpu_reference_time(n_sample, max(1, steps), max(1, min(warmup, 3)), threads)
+    bytes_per = sum(3 * n_sample * s for _, s in DTYPES)
+    gbs = bytes_per / sec / 1e9
+    sample = (f"reduce+inclusive_scan over 2^24 elements of each of f32/f64/i32 (1/16 of the 2^28 workload), "
+              f"{threads} threads, partitioned like reduce.cu/scan.cu")
+    return {"metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": 0, "steps": steps, "warmup": warmup,
+            "ms_per_step": sec * 1e3 * (N_HEADLINE / n_sample), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64+i32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "n": N_HEADLINE, "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# --------------------------------------------------------------------------
+def make_inputs(device, n):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(0)
+    xs = {
+        "f32": torch.rand(n, generator=g, device=device, dtype=torch.float32) * 2 - 1,
+        "f64": torch.rand(n, generator=g, device=device, dtype=torch.float64) * 2 - 1,
+        "i32": torch.randint(-100, 101, (n,), generator=g, device=device, dtype=torch.int32),
+    }
+    return xs
+
+
+def headline(args, device, rank, world):
+    import torch
+    import torch.distributed as dist
+
+    import bulk_b200
+
+    n = args.n
+    xs = make_inputs(device, n)
+    outs = {k: torch.empty_like(v) for k, v in xs.items()}
+    reds = {k: torch.empty(1, dtype=v.dtype, device=device) for k, v in xs.items()}
+    stream = torch.cuda.current_stream(device)
+    # per-call events, recorded on the launching stream
+    ev = {(k, op): [] for k, _ in DTYPES for op in ("reduce", "scan")}
+
+    def step(record):
+        for k, _ in DTYPES:
+            if record:
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            bulk_b200.reduce(xs[k], 0, out=reds[k])
+            if record:
+                b.record(stream)
+                ev[(k, "reduce")].append((a, b))
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            bulk_b200.inclusive_scan(xs[k], 0, out=outs[k])
+            if record:
+                b.record(stream)
+                ev[(k, "scan")].append((a, b))
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    if bulk_b200.workspace_status() != 0:
+        raise RuntimeError("device-side error during warm-up")
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            step(True)
+        end.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    if bulk_b200.workspace_status() != 0:
+        raise RuntimeError("device-side error during the timed region")
+    per = {key: statistics.mean(a.elapsed_time(b) for a, b in lst) for key, lst in ev.items()}
+    return ms, per, clk.summary(), xs
+
+
+def e2e(args, device, xs):
+    """Same workload through the public API with host buffers (pinned), copies timed."""
+    import torch
+
+    import bulk_b200
+    stream = torch.cuda.current_stream(device)
+    h_in = {k: v.cpu().pin_memory() for k, v in xs.items()}
+    h_scan = {k: torch.empty_like(v, device="cpu").pin_memory() for k, v in xs.items()}
+    h_red = {k: torch.empty(1, dtype=v.dtype).pin_memory() for k, v in xs.items()}
+    d_in = {k: torch.empty_like(v) for k, v in xs.items()}
+    d_out = {k: torch.empty_like(v) for k, v in xs.items()}
+    d_red = {k: torch.empty(1, dtype=v.dtype, device=device) for k, v in xs.items()}
+    h2d = sum(v.numel() * v.element_size() for v in h_in.values())
+    d2h = sum(v.numel() * v.element_size() for v in h_scan.values()) + sum(v.element_size() for v in h_red.values())
+
+    def step():
+        for k, _ in DTYPES:
+            d_in[k].copy_(h_in[k], non_blocking=True)
+            bulk_b200.reduce(d_in[k], 0, out=d_red[k])
+            bulk_b200.inclusive_scan(d_in[k], 0, out=d_out[k])
+            h_red[k].copy_(d_red[k], non_blocking=True)
+            h_scan[k].copy_(d_out[k], non_blocking=True)
+
+    steps = max(1, min(args.steps, args.e2e_steps))
+    for _ in range(min(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps, h2d, d2h, steps
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_HEADLINE, help=argparse.SUPPRESS)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    import bulk_b200  # noqa: F401  (fails loudly without the CUDA library)
+
+    ms, per, clocks, xs = headline(args, device, rank, world)
+    ms_step = ms / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    n = args.n
+    bytes_step = sum(3 * n * s for _, s in DTYPES)
+    value = bytes_step * world / (ms_step * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+
+    # dominant kernel: the call with the largest mean time
+    algo_bytes = {(k, "reduce"): n * s for k, s in DTYPES}
+    algo_bytes.update({(k, "scan"): 2 * n * s for k, s in DTYPES})
+    dom = max(per, key=per.get)
+    ops = {f"{op}_{k}": {"GBps": algo_bytes[(k, op)] / (per[(k, op)] * 1e-3) / 1e9,
+                         "ms": per[(k, op)],
+                         "frac_of_hbm": algo_bytes[(k, op)] / (per[(k, op)] * 1e-3) / 1e9 / peak}
+           for (k, op) in per}
+    e2e_ms, h2d, d2h, e2e_steps = e2e(args, device, xs)
+    del xs
+    torch.cuda.empty_cache()
+
+    line = None
+    if rank == 0:
+        achieved = algo_bytes[dom] / (per[dom] * 1e-3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64+i32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": n, "calls_per_step": 6, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (1-2 GiB per array), no flush"},
+            "frac_of_hbm_peak": value / world / peak,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "kernel": f"{dom[1]}_{dom[0]}", "algorithmic_bytes_per_launch": algo_bytes[dom],
+                         "traffic": None},
+            "ops": ops,
+            "e2e": {"value": bytes_step / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps},
+            "gpu_launches": args.steps * 9,
+            "clocks": clocks,
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            ref = cpu_reference_line(3, 1)
+            line["cpu_baseline"] = ref["cpu_baseline"]
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,162 @@
+"""Device-wide algorithms over torch CUDA tensors, calling the C-ABI.
+
+These mirror the reference's device-wide drivers (their names, argument
+meaning and in-place behaviour) so tests and benchmarks read like the
+reference's own drivers:
+
+=====================  ======================================================
+this module            reference (jaredhoberock/bulk)
+=====================  ======================================================
+``reduce``             ``my_reduce(first, last, init, op)``  reduce.cu:58-97
+``inclusive_scan``     ``::inclusive_scan(first, last, result, init, op)``
+                       scan.cu:87-148
+``merge``              ``my_merge(first1, last1, first2, last2, result, comp)``
+                       merge.cu:127-162 (+ by-key block merge merge.hpp:507-607)
+``stable_sort_by_key`` ``stable_merge_sort_by_key(keys_first, keys_last,
+                       values_first, comp)`` merge_sort_by_key.cu:150-209
+``reduce_by_key``      ``my_reduce_by_key(keys_first, keys_last, values_first,
+                       keys_result, values_result, pred, op)``
+                       reduce_by_key.cu:176-272
+=====================  ======================================================
+
+torch provides device memory and streams only; every computation runs in
+libbulkb200.so.  Errors raise :class:`bulk_b200.BulkError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import torch
+
+from . import _lib
+from ._lib import check, lib
+
+_TORCH_TO_TAG = {
+    torch.int32: "i32",
+    torch.int64: "i64",
+    torch.float32: "f32",
+    torch.float64: "f64",
+}
+for _name, _tag in (("uint32", "u32"), ("uint64", "u64")):
+    if hasattr(torch, _name):
+        _TORCH_TO_TAG[getattr(torch, _name)] = _tag
+
+
+def dtype_tag(t: torch.dtype) -> str:
+    try:
+        return _TORCH_TO_TAG[t]
+    except KeyError:
+        raise TypeError(f"unsupported dtype {t}") from None
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream_handle(stream: torch.cuda.Stream | None, device: torch.device) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream(device)
+    return s.cuda_stream
+
+
+def _require_cuda(*ts: torch.Tensor) -> torch.device:
+    dev = None
+    for t in ts:
+        if t is None:
+            continue
+        if not t.is_cuda:
+            raise ValueError("bulk_b200 operates on CUDA tensors (device memory)")
+        if not t.is_contiguous():
+            raise ValueError("bulk_b200 needs contiguous tensors")
+        if dev is None:
+            dev = t.device
+        elif t.device != dev:
+            raise ValueError("all tensors must be on the same device")
+    return dev
+
+
+class _WorkspacePool:
+    """One zero-initialised device workspace per (device, stream), grown on demand.
+
+    The library leaves every workspace's counters zeroed after each call, so a
+    workspace is reused across calls on the same stream without re-clearing.
+    """
+
+    def __init__(self):
+        self._lock = threading.Lock()
+        self._ws: dict[tuple[int, int], torch.Tensor] = {}
+
+    def get(self, nbytes: int, device: torch.device, stream: int) -> tuple[int, int]:
+        key = (device.index if device.index is not None else torch.cuda.current_device(), stream)
+        with self._lock:
+            t = self._ws.get(key)
+            if t is None or t.numel() < nbytes:
+                size = max(nbytes, 1 << 16, 0 if t is None else 2 * t.numel())
+                t = torch.zeros(size, dtype=torch.uint8, device=device)
+                self._ws[key] = t
+            return t.data_ptr(), t.numel()
+
+    def status(self, device: torch.device | None = None, stream: torch.cuda.Stream | None = None) -> int:
+        device = device or torch.device("cuda", torch.cuda.current_device())
+        s = _stream_handle(stream, device)
+        key = (device.index if device.index is not None else torch.cuda.current_device(), s)
+        t = self._ws.get(key)
+        if t is None:
+            return _lib.BK_OK
+        return lib.bk_workspace_status(t.data_ptr(), t.numel(), s)
+
+    def clear(self):
+        with self._lock:
+            self._ws.clear()
+
+
+workspaces = _WorkspacePool()
+
+
+def workspace_bytes(algo: str, key: str, value: str | None, n: int) -> int:
+    return lib.bk_workspace_bytes(_lib.ALGO[algo], _lib.DTYPE[key], _lib.DTYPE[value], n)
+
+
+def workspace_status(device=None, stream=None) -> int:
+    """Synchronize and return (and clear) the device-side status of this stream's workspace."""
+    return workspaces.status(device, stream)
+
+
+def debug_set_fault(skip_publish_tile: int = -1, spin_limit_ns: int = 0) -> None:
+    check(lib.bk_debug_set_fault(skip_publish_tile, spin_limit_ns), "bk_debug_set_fault")
+
+
+def _ws(algo, key, value, n, device, stream):
+    need = workspace_bytes(algo, key, value, n)
+    if need == 0 and algo not in ("reduce",):
+        return None, 0
+    return workspaces.get(max(need, 256), device, stream)
+
+
+# ---------------------------------------------------------------------------
+def reduce(x: torch.Tensor, init=0, op: str = "sum", out: torch.Tensor | None = None,
+           stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """Return a 1-element device tensor holding init (+) x[0] (+) ... (+) x[n-1]."""
+    dev = _require_cuda(x, out)
+    tag = dtype_tag(x.dtype)
+    if out is None:
+        out = torch.empty(1, dtype=x.dtype, device=dev)
+    s = _stream_handle(stream, dev)
+    ws, wsb = _ws("reduce", tag, None, x.numel(), dev, s)
+    fn = getattr(lib, f"bk_reduce_{op}_{tag}")
+    check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
+    return out
+
+
+def inclusive_scan(x: torch.Tensor, init=0, op: str = "sum", out: torch.Tensor | None = None,
+                   stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """out[i] = init (+) x[0] (+) ... (+) x[i]; ``out`` may be ``x`` (in place)."""
+    dev = _require_cuda(x, out)
+    tag = dtype_tag(x.dtype)
+    if out is None:
+        out = torch.empty_like(x)
+    s = _stream_handle(stream, dev)
+    ws, wsb = _ws("inclusive_scan", tag, None, x.numel(), dev, s)
+    fn = getattr(lib, f"bk_inclusive_scan_{op}_{tag}")
+    check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
+    return out

@@ -1,0 +1,102 @@
+"""Build libbulkb200.so (the C-ABI library) in-tree with nvcc for sm_100a.
+
+Each ``csrc/*.cu`` file is compiled separately (in parallel) with
+``-gencode arch=compute_100a,code=sm_100a -lineinfo`` and the objects are
+linked into ``bulk_b200/lib/libbulkb200.so`` against the static CUDA runtime,
+so the library carries no dependency on a particular libcudart.so.
+
+Usage: ``python -m bulk_b200.build [--force] [--verbose]``.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIBDIR = PKG / "lib"
+LIB = LIBDIR / "libbulkb200.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [
+    "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC,-O3,-fvisibility=hidden",
+    "-Xptxas", "-v",
+    f"-I{ROOT / 'include'}", f"-I{CSRC}",
+]
+
+
+def nvcc() -> str:
+    cand = os.environ.get("NVCC") or shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build bulk_b200")
+    return cand
+
+
+def _sources() -> list[Path]:
+    return sorted(CSRC.glob("*.cu"))
+
+
+def _deps() -> list[Path]:
+    return sorted(CSRC.glob("*.cuh")) + sorted((ROOT / "include").glob("*.h")) + [Path(__file__)]
+
+
+def _needs(target: Path, inputs: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in inputs)
+
+
+def _compile(src: Path, verbose: bool) -> tuple[Path, str]:
+    obj = BUILD / (src.stem + ".o")
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    log = r.stdout + r.stderr
+    (BUILD / (src.stem + ".ptxas.txt")).write_text(log)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{log[-6000:]}")
+    if verbose:
+        print(log)
+    return obj, log
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    LIBDIR.mkdir(exist_ok=True)
+    deps = _deps()
+    srcs = _sources()
+    todo = [s for s in srcs if force or _needs(BUILD / (s.stem + ".o"), [s, *deps])]
+    if todo:
+        workers = min(len(todo), os.cpu_count() or 4)
+        with cf.ThreadPoolExecutor(workers) as ex:
+            list(ex.map(lambda s: _compile(s, verbose), todo))
+    objs = [BUILD / (s.stem + ".o") for s in srcs]
+    if force or todo or _needs(LIB, objs):
+        tmp = LIB.with_suffix(".so.tmp")
+        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}{r.stderr}")
+        os.replace(tmp, LIB)
+    return LIB
+
+
+def main(argv: list[str] | None = None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    a = ap.parse_args(argv)
+    print(build(force=a.force, verbose=a.verbose))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,143 @@
+/*
+ * bulk_b200.h -- C-ABI of the B200 (sm_100a) device-wide algorithm library.
+ *
+ * Every entry point takes plain device pointers, 64-bit element counts, a
+ * caller-owned device workspace and a CUDA stream, and returns an int status
+ * (BK_OK, a positive cudaError_t value, or a negative BK_ERR_* library code).
+ * Calls are stream-ordered and asynchronous: results stay in device memory and
+ * the caller synchronizes.  No entry point allocates memory.
+ *
+ * Each entry replaces one device-wide driver of the reference library
+ * (jaredhoberock/bulk); the replaced interface is cited above each group as
+ * file:line within that project.
+ *
+ * Workspace contract: query the size with bk_workspace_bytes(), allocate it on
+ * the device, and zero-fill it once (bk_workspace_init or cudaMemset).  Every
+ * call leaves its counters zeroed again.  One workspace serves one stream at a
+ * time: calls that overlap on the device must use different workspaces.
+ * Device-side failures (a look-back wait that ran out) are recorded in the
+ * workspace and returned by bk_workspace_status().
+ */
+#ifndef BULK_B200_H
+#define BULK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BK_API __attribute__((visibility("default")))
+#else
+#define BK_API
+#endif
+
+/* Same underlying type as cudaStream_t; NULL is the legacy default stream. */
+typedef struct CUstream_st *bk_stream_t;
+
+/* ---- status codes ------------------------------------------------------ */
+#define BK_OK 0
+#define BK_ERR_INVALID_ARGUMENT (-1)    /* null pointer with n > 0, bad enum, ... */
+#define BK_ERR_WORKSPACE_TOO_SMALL (-2) /* ws_bytes < bk_workspace_bytes(...)      */
+#define BK_ERR_SPIN_TIMEOUT (-3)        /* a device-side wait hit its time limit   */
+#define BK_ERR_MISALIGNED (-4)          /* pointer not aligned to its element size */
+#define BK_ERR_TOO_LARGE (-5)           /* n beyond the supported maximum          */
+#define BK_ERR_UNSUPPORTED (-6)         /* no sm_100 device / unsupported combo    */
+
+/* ---- enums used by the workspace query ---------------------------------- */
+#define BK_ALGO_REDUCE 1
+#define BK_ALGO_INCLUSIVE_SCAN 2
+#define BK_ALGO_MERGE 3
+#define BK_ALGO_SORT_BY_KEY 4
+#define BK_ALGO_REDUCE_BY_KEY 5
+
+#define BK_DTYPE_NONE 0
+#define BK_DTYPE_I32 1
+#define BK_DTYPE_U32 2
+#define BK_DTYPE_I64 3
+#define BK_DTYPE_U64 4
+#define BK_DTYPE_F32 5
+#define BK_DTYPE_F64 6
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+BK_API int bk_version(void);
+
+/* Human-readable text for any status this library returns. */
+BK_API const char *bk_status_string(int status);
+
+/* Bytes of device workspace that one call of `algo` over n elements needs.
+ * key_dtype is the element (reduce/scan) or key type; value_dtype is the
+ * payload type (BK_DTYPE_NONE for keys-only / value-less algorithms).
+ * Returns 0 for an unknown combination. */
+BK_API size_t bk_workspace_bytes(int algo, int key_dtype, int value_dtype, uint64_t n);
+
+/* Zero-fill a workspace on `stream` (the one-time initialisation). */
+BK_API int bk_workspace_init(void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
+/* Synchronize `stream`, return the device-side status recorded in the
+ * workspace by earlier calls (BK_OK or BK_ERR_SPIN_TIMEOUT) and clear it. */
+BK_API int bk_workspace_status(void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
+/* Test hook (not thread-safe; process-wide).  Subsequent look-back kernels
+ * make the tile with index skip_publish_tile (-1 = none) skip publishing its
+ * status, and bound every look-back wait by spin_limit_ns (0 = default, 2 s).
+ * Waiting tiles then give up, record BK_ERR_SPIN_TIMEOUT and return. */
+BK_API int bk_debug_set_fault(int64_t skip_publish_tile, uint64_t spin_limit_ns);
+
+/* ---- reduce -------------------------------------------------------------
+ * *d_out = init (+) in[0] (+) ... (+) in[n-1]; n == 0 writes init.
+ * Replaces my_reduce(first, last, init, binary_op), reduce.cu:58-97, whose
+ * partition kernel calls bulk::reduce(group, ...), bulk/algorithm/reduce.hpp:110-219.
+ * Integer sums wrap modulo 2^32 / 2^64 like the reference's.  Floating-point
+ * results are reproducible run to run for a given n and device. */
+BK_API int bk_reduce_sum_i32(const int32_t *d_in, uint64_t n, int32_t init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_sum_u32(const uint32_t *d_in, uint64_t n, uint32_t init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_sum_i64(const int64_t *d_in, uint64_t n, int64_t init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_sum_u64(const uint64_t *d_in, uint64_t n, uint64_t init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_sum_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_sum_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_min_i32(const int32_t *d_in, uint64_t n, int32_t init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_min_u32(const uint32_t *d_in, uint64_t n, uint32_t init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_min_i64(const int64_t *d_in, uint64_t n, int64_t init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_min_u64(const uint64_t *d_in, uint64_t n, uint64_t init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_min_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_min_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_max_i32(const int32_t *d_in, uint64_t n, int32_t init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_max_u32(const uint32_t *d_in, uint64_t n, uint32_t init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_max_i64(const int64_t *d_in, uint64_t n, int64_t init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_max_u64(const uint64_t *d_in, uint64_t n, uint64_t init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_max_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_max_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
+/* ---- inclusive scan -----------------------------------------------------
+ * d_out[i] = init (+) in[0] (+) ... (+) in[i]; in-place (d_out == d_in) is allowed.
+ * Replaces ::inclusive_scan(first, last, result, init, binary_op), scan.cu:87-148
+ * (upsweep accumulate_tiles :57-84, spine exclusive_scan_n :24-31, downsweep
+ * inclusive_downsweep :34-54, which call bulk::inclusive_scan(group, ...),
+ * bulk/algorithm/scan.hpp:455-486), as one single-pass look-back kernel. */
+BK_API int bk_inclusive_scan_sum_i32(const int32_t *d_in, uint64_t n, int32_t init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_u32(const uint32_t *d_in, uint64_t n, uint32_t init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_i64(const int64_t *d_in, uint64_t n, int64_t init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_u64(const uint64_t *d_in, uint64_t n, uint64_t init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_i32(const int32_t *d_in, uint64_t n, int32_t init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_u32(const uint32_t *d_in, uint64_t n, uint32_t init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_i64(const int64_t *d_in, uint64_t n, int64_t init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_u64(const uint64_t *d_in, uint64_t n, uint64_t init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_i32(const int32_t *d_in, uint64_t n, int32_t init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_u32(const uint32_t *d_in, uint64_t n, uint32_t init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_i64(const int64_t *d_in, uint64_t n, int64_t init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_u64(const uint64_t *d_in, uint64_t n, uint64_t init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* BULK_B200_H */
