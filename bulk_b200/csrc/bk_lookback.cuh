@@ -1,15 +1,24 @@
 // bk_lookback.cuh -- single-pass decoupled look-back across CTAs.
 //
-// Each tile of a single-pass scan publishes its status in a per-tile word:
+// Each tile of a single-pass scan publishes its status in a per-tile slot:
 //   INVALID   nothing yet
 //   AGGREGATE the tile's own reduction (published as soon as it is known)
 //   PREFIX    the inclusive prefix through this tile
-// A tile's warp 0 reads the 32 nearest predecessors at once, folds the
-// aggregates up to the nearest PREFIX, and slides the window back while none
-// is found.  Tiles are handed out by an atomic ticket in launch order, so every
-// predecessor a tile waits on is already running: the wait always ends.  Each
-// wait is still bounded (globaltimer), and on expiry the kernel records
-// BK_ERR_SPIN_TIMEOUT in the workspace header and returns instead of hanging.
+// A payload of W 32-bit words occupies W 64-bit status words, each holding
+// (tag << 32 | data word); tag 0 = INVALID, 1 = AGGREGATE, 2 = PREFIX.  Every
+// 64-bit word is stored and loaded single-copy atomically, so a reader that
+// sees the same non-zero tag in all W words holds a consistent payload (each
+// tag is written at most once per call); mixed tags mean a write in progress
+// and the reader looks again.  A slot is therefore read in one L2 round trip,
+// with no fences.
+//
+// Warp 0 of a tile reads kLbPerLane x 32 predecessors per round, folds the
+// aggregates up to the nearest PREFIX (in order, so non-commutative operators
+// work) and slides the window back while none is found.  Tiles are handed out
+// by an atomic ticket in launch order, so every predecessor a tile waits on is
+// already running: the wait always ends.  Each wait is still bounded
+// (globaltimer); on expiry the kernel records BK_ERR_SPIN_TIMEOUT in the
+// workspace header and the tile returns instead of hanging.
 #pragma once
 
 #include "bk_common.cuh"
@@ -17,77 +26,53 @@
 namespace bk {
 
 enum : unsigned int { kStInvalid = 0u, kStAggregate = 1u, kStPrefix = 2u, kStError = 3u };
-
-// Payloads of 4 bytes share one 64-bit word with their flag (single-copy
-// atomic store/load).  Larger payloads (8 or 16 bytes) use a flag array plus
-// separate aggregate / prefix arrays ordered by release/acquire.
-template <typename P, bool kPacked = (sizeof(P) == 4)>
-struct TileStatus;
+constexpr int kLbPerLane = 4;  // predecessors read per lane per round (128 per warp)
 
 template <typename P>
-struct TileStatus<P, true> {
+struct TileStatus {
+  static_assert(sizeof(P) % 4 == 0 && sizeof(P) <= 16, "payload of 4, 8, 12 or 16 bytes");
+  static constexpr int W = sizeof(P) / 4;  // 32-bit payload words = 64-bit status words per tile
   unsigned long long *words;
 
-  __host__ __device__ static size_t bytes(size_t tiles) { return align_up(tiles * 8, 256); }
+  // Rounded up to whole groups of kLbPerLane tiles (the look-back reads groups).
+  __host__ __device__ static size_t bytes(size_t tiles) { return align_up(align_up(tiles, 4) * W * 8, 256); }
   __host__ __device__ static TileStatus at(void *base, size_t /*tiles*/) {
     return TileStatus{reinterpret_cast<unsigned long long *>(base)};
   }
 
   __device__ __forceinline__ void publish(unsigned int tile, unsigned int flag, P v) const {
-    st_relaxed_u64(words + tile, ((unsigned long long)flag << 32) | (unsigned long long)bit_cast<uint32_t>(v));
-  }
-  __device__ __forceinline__ unsigned int read(unsigned int tile, P &v) const {
-    unsigned long long w = ld_relaxed_u64(words + tile);
-    v = bit_cast<P>((uint32_t)(w & 0xffffffffull));
-    return (unsigned int)(w >> 32);
-  }
-  // Zero `tiles` words; called by the init kernel.
-  __device__ __forceinline__ void clear(size_t i) const { words[i] = 0ull; }
-};
-
-template <typename P>
-struct TileStatus<P, false> {
-  static_assert(sizeof(P) % 8 == 0 && sizeof(P) <= 16, "payload of 8 or 16 bytes");
-  static constexpr int kWords = sizeof(P) / 8;
-  unsigned int *flags;
-  unsigned long long *agg;
-  unsigned long long *incl;
-
-  __host__ __device__ static size_t bytes(size_t tiles) {
-    return align_up(tiles * 4, 256) + 2 * align_up(tiles * sizeof(P), 256);
-  }
-  __host__ __device__ static TileStatus at(void *base, size_t tiles) {
-    char *b = reinterpret_cast<char *>(base);
-    TileStatus s;
-    s.flags = reinterpret_cast<unsigned int *>(b);
-    s.agg = reinterpret_cast<unsigned long long *>(b + align_up(tiles * 4, 256));
-    s.incl = reinterpret_cast<unsigned long long *>(b + align_up(tiles * 4, 256) + align_up(tiles * sizeof(P), 256));
-    return s;
-  }
-  __device__ __forceinline__ void publish(unsigned int tile, unsigned int flag, P v) const {
-    unsigned long long w[kWords];
-    memcpy(w, &v, sizeof(P));
-    unsigned long long *dst = (flag == kStAggregate ? agg : incl) + (size_t)tile * kWords;
+    uint32_t d[W];
+    memcpy(d, &v, sizeof(P));
+    unsigned long long *dst = words + (size_t)tile * W;
+    const unsigned long long tag = (unsigned long long)flag << 32;
 #pragma unroll
-    for (int i = 0; i < kWords; ++i) st_relaxed_u64(dst + i, w[i]);
-    st_release_u32(flags + tile, flag);  // orders the payload before the flag
+    for (int i = 0; i < W; ++i) st_relaxed_u64(dst + i, tag | d[i]);
   }
+  // Returns INVALID while the slot is empty or being written.
   __device__ __forceinline__ unsigned int read(unsigned int tile, P &v) const {
-    unsigned int f = ld_acquire_u32(flags + tile);
-    if (f == kStAggregate || f == kStPrefix) {
-      const unsigned long long *src = (f == kStAggregate ? agg : incl) + (size_t)tile * kWords;
-      unsigned long long w[kWords];
+    const unsigned long long *src = words + (size_t)tile * W;
+    unsigned long long w[W];
 #pragma unroll
-      for (int i = 0; i < kWords; ++i) w[i] = ld_relaxed_u64(src + i);
-      memcpy(&v, w, sizeof(P));
-    }
+    for (int i = 0; i < W; ++i) w[i] = ld_relaxed_u64(src + i);
+    const unsigned int f = (unsigned int)(w[0] >> 32);
+    bool same = true;
+#pragma unroll
+    for (int i = 1; i < W; ++i) same &= ((unsigned int)(w[i] >> 32) == f);
+    if (!same) return kStInvalid;
+    uint32_t d[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) d[i] = (uint32_t)(w[i] & 0xffffffffull);
+    memcpy(&v, d, sizeof(P));
     return f;
   }
-  __device__ __forceinline__ void clear(size_t i) const { flags[i] = 0u; }
+  __device__ __forceinline__ void clear(size_t tile) const {
+#pragma unroll
+    for (int i = 0; i < W; ++i) words[tile * W + i] = 0ull;
+  }
 };
 
 // Ordered warp reduction: lane 0 receives v[31] (+) ... (+) v[1] (+) v[0]
-// (higher lanes are earlier tiles), valid for non-commutative operators.
+// (higher lanes hold earlier tiles), valid for non-commutative operators.
 template <typename P, typename Op>
 __device__ __forceinline__ P warp_reduce_ordered(P v, Op op, int lane) {
 #pragma unroll
@@ -98,50 +83,120 @@ __device__ __forceinline__ P warp_reduce_ordered(P v, Op op, int lane) {
   return v;
 }
 
+// Spin (bounded) until the status of `tile` is valid.  Returns the flag, or
+// kStError when the wait ran out or another tile already failed.
+template <typename P, typename Status>
+__device__ __forceinline__ unsigned int wait_status(const Status &st, unsigned int tile, P &v, WsHeader *hdr,
+                                                    unsigned long long limit_ns, unsigned long long &t0) {
+  unsigned int spins = 0;
+  while (true) {
+    const unsigned int f = st.read(tile, v);
+    if (f != kStInvalid) return f;
+    ++spins;
+    if ((spins & 15u) == 0) {
+      const unsigned long long now = globaltimer_ns();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > limit_ns || ld_relaxed_s32(&hdr->status) != 0) {
+        return kStError;
+      }
+    }
+    if (spins > 4) __nanosleep(spins < 128 ? 20 : 200);
+  }
+}
+
 // Warp 0 of tile `tile` (> 0) computes the exclusive prefix of all earlier
 // tiles.  Returns false (after recording the error) when a wait ran out or
-// another tile already failed.
+// another tile already failed.  All 32 lanes must call it.
+//
+// Lane l reads the aligned group of kLbPerLane tiles g = G - l, where G is the
+// group holding tile - 1: one or more 16-byte vector loads per lane, all issued
+// before any result is used.  Tiles at or after `tile` in the first group do
+// not take part.
 template <typename P, typename Op, typename Status>
 __device__ __forceinline__ bool lookback_exclusive(const Status &st, unsigned int tile, Op op, P &exclusive,
                                                    WsHeader *hdr, unsigned long long limit_ns) {
+  constexpr int K = kLbPerLane;
+  constexpr int W = Status::W;
+  constexpr int GW = K * W;  // 64-bit words per group (even: K is 4)
+  static_assert(GW % 2 == 0, "group is a whole number of 16-byte vectors");
   const int lane = threadIdx.x & 31;
-  long long pred = (long long)tile - 1;
+  long long group = ((long long)tile - 1) / K - lane;
   P acc = Op::identity();
   unsigned long long t0 = 0;
   while (true) {
-    const long long idx = pred - lane;
-    P v = Op::identity();
-    unsigned int f = kStPrefix;  // indices below 0 never occur: tile 0 always publishes PREFIX
-    if (idx >= 0) {
-      unsigned int spins = 0;
-      while (true) {
-        f = st.read((unsigned int)idx, v);
-        if (f != kStInvalid) break;
-        ++spins;
-        if ((spins & 31u) == 0) {
-          unsigned long long now = globaltimer_ns();
-          if (t0 == 0) {
-            t0 = now;
-          } else if (now - t0 > limit_ns || ld_relaxed_s32(&hdr->status) != 0) {
-            f = kStError;
-            break;
-          }
+    // ---- read the group (tiles 4g .. 4g+3; j = 0 is the nearest = 4g+3)
+    P v[K];
+    unsigned int f[K];
+    if (group >= 0) {
+      unsigned long long w[GW];
+      const unsigned long long *src = st.words + (size_t)group * GW;
+#pragma unroll
+      for (int i = 0; i < GW; i += 2) ld_relaxed_v2_u64(src + i, w[i], w[i + 1]);
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const int t = K - 1 - j;  // position within the group
+        const unsigned int tag = (unsigned int)(w[t * W] >> 32);
+        bool same = true;
+        uint32_t d[W];
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+          same &= ((unsigned int)(w[t * W + i] >> 32) == tag);
+          d[i] = (uint32_t)(w[t * W + i] & 0xffffffffull);
         }
-        if (spins > 8) __nanosleep(spins < 256 ? 32 : 256);
+        f[j] = same ? tag : kStInvalid;
+        memcpy(&v[j], d, sizeof(P));
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        f[j] = kStPrefix;  // before tile 0: never chosen, tile 0 always publishes PREFIX
+        v[j] = Op::identity();
       }
     }
-    if (__any_sync(0xffffffffu, f == kStError)) {
+    // tiles at or after `tile` (first round, lane 0 only) do not take part
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const long long idx = group * K + (K - 1 - j);
+      if (idx >= (long long)tile) {
+        f[j] = kStAggregate;
+        v[j] = Op::identity();
+      }
+    }
+    // ---- wait for any not yet valid (nearest first)
+    bool err = false;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const long long idx = group * K + (K - 1 - j);
+      if (group >= 0 && f[j] == kStInvalid && !err) {
+        f[j] = wait_status(st, (unsigned int)idx, v[j], hdr, limit_ns, t0);
+        err |= (f[j] == kStError);
+      }
+    }
+    if (__any_sync(0xffffffffu, err)) {
       if (lane == 0) record_error(hdr, BK_ERR_SPIN_TIMEOUT, tile);
       return false;
     }
-    const unsigned int pmask = __ballot_sync(0xffffffffu, f == kStPrefix);
-    const int stop = pmask ? (__ffs(pmask) - 1) : 31;
-    if (lane > stop) v = Op::identity();
-    P w = warp_reduce_ordered(v, op, lane);
-    w = shfl_idx_any(w, 0);
-    acc = op(w, acc);
+    // ---- nearest PREFIX: in the lowest lane that has one, at its lowest j
+    int first_j = K;
+#pragma unroll
+    for (int j = K - 1; j >= 0; --j)
+      if (f[j] == kStPrefix) first_j = j;
+    const unsigned int pmask = __ballot_sync(0xffffffffu, first_j < K);
+    const int stop_lane = pmask ? (__ffs(pmask) - 1) : 32;
+    // lane-local ordered fold (farthest first), truncated at the PREFIX
+    P lv = Op::identity();
+    if (lane <= stop_lane) {
+      const int last = (lane == stop_lane) ? first_j : K - 1;
+#pragma unroll
+      for (int j = K - 1; j >= 0; --j)
+        if (j <= last) lv = op(lv, v[j]);
+    }
+    P wsum = warp_reduce_ordered(lv, op, lane);
+    wsum = shfl_idx_any(wsum, 0);
+    acc = op(wsum, acc);
     if (pmask) break;
-    pred -= 32;
+    group -= 32;
   }
   exclusive = acc;
   return true;

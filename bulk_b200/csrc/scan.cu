@@ -6,29 +6,32 @@
 // bulk/algorithm/scan.hpp:222-384.  That design moves 3*N*s bytes; this one
 // moves the minimum 2*N*s (read once, write once).
 //
-// Per tile (THREADS x ITEMS elements, 16 KB): an atomic ticket names the tile
-// (launch order, so every predecessor is already running); each thread loads
-// ITEMS contiguous elements with 16-byte vector loads, scans them serially in
-// registers, the CTA scans the per-thread totals with warp shuffles, the tile
-// publishes its aggregate, warp 0 looks back over its predecessors for the
-// exclusive prefix (bk_lookback.cuh), publishes the inclusive prefix, and the
-// threads write their outputs with 16-byte streaming stores.  A tiny init
-// kernel clears the tile status words before each scan.
+// Per tile (32 KB): an atomic ticket names the tile (launch order, so every
+// predecessor is already running); one TMA bulk copy brings the tile into
+// shared memory; each warp scans its rows of 16-byte chunks with shuffles;
+// the tile publishes its aggregate, warp 0 looks back over its predecessors
+// for the exclusive prefix (bk_lookback.cuh) and publishes the inclusive
+// prefix; the results leave with one TMA bulk store.  A tiny init kernel
+// clears the tile status words before each scan.
 //
 // Semantics follow scan.cu:166-169 and bulk/algorithm/scan.hpp:455-486:
 // out[i] = init (+) in[0] (+) ... (+) in[i].
 #include "bk_common.cuh"
 #include "bk_lookback.cuh"
+#include "bk_tma.cuh"
 
 namespace bk {
 
 constexpr int kScanThreads = 256;
+constexpr int kScanWarps = kScanThreads / 32;
+constexpr int kScanRowsPerWarp = 8;
 
 template <typename T>
 struct ScanCfg {
-  static constexpr int ITEMS = 64 / sizeof(T);  // 16 for 4-byte, 8 for 8-byte types
-  static constexpr int TILE = kScanThreads * ITEMS;
-  static constexpr int V = 16 / sizeof(T);
+  static constexpr int V = 16 / sizeof(T);                              // elements per 16-byte chunk
+  static constexpr int ROW = 32 * V;                                    // elements per warp row
+  static constexpr int TILE = kScanWarps * kScanRowsPerWarp * ROW;     // 8192 (4 B) / 4096 (8 B)
+  static constexpr int TILE_BYTES = TILE * (int)sizeof(T);              // 32 KB
   using Status = TileStatus<T>;
 };
 
@@ -52,94 +55,284 @@ template <typename Status>
 __global__ void lookback_init_kernel(Status st, size_t tiles, WsHeader *hdr) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t t = i; t < tiles; t += stride) st.clear(t);
+  const size_t padded = align_up(tiles, 4);  // whole look-back groups
+  for (size_t t = i; t < padded; t += stride) st.clear(t);
   if (i == 0) hdr->tile_ticket = 0u;
 }
 
-template <typename T, typename Op>
-__global__ void __launch_bounds__(kScanThreads, 5) scan_kernel(const T *in, T *out, uint64_t n, T init,
-                                                            typename ScanCfg<T>::Status st, WsHeader *hdr,
-                                                            unsigned long long spin_limit_ns,
-                                                            long long skip_publish_tile, int vec_ok) {
+// Copies tile `tile` of `src` into shared memory `buf`: the 16-byte-aligned
+// body with one TMA bulk copy completing on `bar` (returns whether one was
+// issued), the ragged tail (fewer than V elements) with plain loads by the
+// calling thread.  Called by one thread.
+template <typename T>
+__device__ __forceinline__ bool scan_issue_tile_load(const T *src, uint64_t n, unsigned int tile, T *buf,
+                                                     uint64_t *bar, uint64_t policy) {
   using C = ScanCfg<T>;
-  constexpr int ITEMS = C::ITEMS, TILE = C::TILE, V = C::V;
+  const uint64_t base = (uint64_t)tile * C::TILE;
+  const uint32_t count = (uint32_t)((n - base) < (uint64_t)C::TILE ? (n - base) : (uint64_t)C::TILE);
+  const uint32_t bulk = count & ~(uint32_t)(C::V - 1);
+  for (uint32_t i = bulk; i < count; ++i) buf[i] = src[base + i];
+  if (bulk == 0) return false;
+  mbar_arrive_expect_tx(bar, bulk * (uint32_t)sizeof(T));
+  tma_load_1d_hint(buf, src + base, bulk * (uint32_t)sizeof(T), bar, policy);
+  return true;
+}
+
+// All threads: plain coalesced copy of a tile into shared memory (used when
+// the pointers are not 16-byte aligned).
+template <typename T>
+__device__ __forceinline__ void scan_sync_tile_load(const T *src, uint64_t n, unsigned int tile, T *buf) {
+  using C = ScanCfg<T>;
+  const uint64_t base = (uint64_t)tile * C::TILE;
+  const uint32_t count = (uint32_t)((n - base) < (uint64_t)C::TILE ? (n - base) : (uint64_t)C::TILE);
+  for (uint32_t i = threadIdx.x; i < count; i += kScanThreads) buf[i] = src[base + i];
+}
+
+template <typename T>
+__device__ __forceinline__ uint32_t scan_tile_count(uint64_t n, unsigned int tile) {
+  const uint64_t base = (uint64_t)tile * ScanCfg<T>::TILE;
+  return (uint32_t)((n - base) < (uint64_t)ScanCfg<T>::TILE ? (n - base) : (uint64_t)ScanCfg<T>::TILE);
+}
+
+// Persistent two-phase scan.  Each CTA loops over tiles taken from an atomic
+// ticket.  Iteration i of a CTA:
+//   * takes the ticket of its next tile and starts its TMA load (kept in L2
+//     with an evict-last hint) -- one tile ahead;
+//   * starts re-reading its previous tile p from L2 (evict-first);
+//   * phase 1 of the current tile t: reduce it (pass A) and publish its
+//     aggregate (tile 0 publishes its inclusive prefix at once);
+//   * phase 2 of p: warp 0 looks back for p's exclusive prefix -- by now every
+//     predecessor's aggregate is an iteration old, so nothing waits on a slow
+//     load -- while the other warps scan p's rows (pass B); then pass C adds
+//     the prefix and one TMA bulk store writes the tile out (evict-first).
+// A tile waiting for its prefix holds no shared memory: its data waits in L2.
+// Every wait points at a lower tile whose ticket a running CTA already took,
+// so the waits always end; each is still bounded by spin_limit_ns.
+template <typename T, typename Op>
+__global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *out, uint64_t n, T init,
+                                                               typename ScanCfg<T>::Status st, WsHeader *hdr,
+                                                               unsigned long long spin_limit_ns,
+                                                               long long skip_publish_tile, int tma_ok,
+                                                               unsigned int num_tiles) {
+  using C = ScanCfg<T>;
+  constexpr int V = C::V, TILE = C::TILE, R = kScanRowsPerWarp;
+  constexpr unsigned int NONE = 0xffffffffu;
   Op op;
-  __shared__ unsigned int s_tile;
-  __shared__ T s_warp[kScanThreads / 32 + 1];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T *const bufA0 = reinterpret_cast<T *>(smem_raw);
+  T *const bufA1 = bufA0 + TILE;
+  T *const bufB = bufA1 + TILE;
+  __shared__ __align__(8) uint64_t s_bar[3];  // 0, 1: phase-1 slots; 2: phase-2 buffer
+  __shared__ unsigned int s_ticket[2];
+  __shared__ int s_has_tma[3];
+  __shared__ T s_wtot[2][kScanWarps];
   __shared__ T s_prefix;
   __shared__ int s_abort;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t keep = l2_policy_evict_last();
+  const uint64_t stream = l2_policy_evict_first();
 
   if (tid == 0) {
-    s_tile = atomicAdd(&hdr->tile_ticket, 1u);
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    mbar_init(&s_bar[2], 1);
+    fence_proxy_async_smem();
     s_abort = 0;
+    s_has_tma[0] = s_has_tma[1] = s_has_tma[2] = 0;
+    const unsigned int t0 = atomicAdd(&hdr->tile_ticket, 1u);
+    s_ticket[0] = t0 < num_tiles ? t0 : NONE;
+    if (t0 < num_tiles && tma_ok) s_has_tma[0] = scan_issue_tile_load(in, n, t0, bufA0, &s_bar[0], keep);
   }
   __syncthreads();
-  const unsigned int tile = s_tile;
-  const uint64_t base = (uint64_t)tile * TILE;
-  const uint64_t my0 = base + (uint64_t)tid * ITEMS;
-  const bool full = (base + TILE <= n);
 
-  T x[ITEMS];
-  if (full && vec_ok) {
-#pragma unroll
-    for (int k = 0; k < ITEMS / V; ++k) {
-      uint4 r;
-      asm("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
-          : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
-          : "l"(in + my0 + k * V));
-      memcpy(&x[k * V], &r, 16);
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) x[i] = (my0 + i < n) ? in[my0 + i] : Op::identity();
-  }
+  uint32_t parity[3] = {0u, 0u, 0u};
+  uint32_t inflight = s_has_tma[0] ? 1u : 0u;  // bit b: a TMA load on s_bar[b] not yet waited for
+  unsigned int pending = NONE;  // tile whose phase 2 is due this iteration
+  T pending_agg = Op::identity();
+  bool issued_store = false;
 
-  // Thread-local inclusive scan.
-#pragma unroll
-  for (int i = 1; i < ITEMS; ++i) x[i] = op(x[i - 1], x[i]);
+  for (int it = 0;; ++it) {
+    const int slot = it & 1;
+    const unsigned int t = s_ticket[slot];
+    T *const bA = slot ? bufA1 : bufA0;
+    T *const bA_next = slot ? bufA0 : bufA1;
 
-  T aggregate;
-  const T thread_excl = block_exclusive_scan<kScanThreads>(x[ITEMS - 1], op, s_warp, aggregate);
-
-  const bool publish = ((long long)tile != skip_publish_tile);
-  if (tile == 0) {
+    // ---- start the loads: next phase-1 tile, and the phase-2 re-read
     if (tid == 0) {
-      if (publish) st.publish(0u, kStPrefix, op(init, aggregate));
-      s_prefix = init;
-    }
-  } else if (tid < 32) {
-    if (tid == 0 && publish) st.publish(tile, kStAggregate, aggregate);
-    T excl;
-    const bool ok = lookback_exclusive<T>(st, tile, op, excl, hdr, spin_limit_ns);
-    if (tid == 0) {
-      if (ok) {
-        if (publish) st.publish(tile, kStPrefix, op(excl, aggregate));
-        s_prefix = excl;
-      } else {
-        s_abort = 1;
+      unsigned int tn = NONE;
+      if (t != NONE) {
+        const unsigned int x = atomicAdd(&hdr->tile_ticket, 1u);
+        if (x < num_tiles) tn = x;
+      }
+      s_ticket[slot ^ 1] = tn;
+      s_has_tma[slot ^ 1] = 0;
+      if (tn != NONE && tma_ok) s_has_tma[slot ^ 1] = scan_issue_tile_load(in, n, tn, bA_next, &s_bar[slot ^ 1], keep);
+      s_has_tma[2] = 0;
+      if (pending != NONE && tma_ok) {
+        if (issued_store) tma_store_wait_read();  // bufB free again
+        s_has_tma[2] = scan_issue_tile_load(in, n, pending, bufB, &s_bar[2], stream);
       }
     }
-  }
-  __syncthreads();
-  if (s_abort) return;
-
-  const T tile_excl = s_prefix;
-  const T carry = (tid == 0) ? tile_excl : op(tile_excl, thread_excl);
-#pragma unroll
-  for (int i = 0; i < ITEMS; ++i) x[i] = op(carry, x[i]);
-
-  if (full && vec_ok) {
-#pragma unroll
-    for (int k = 0; k < ITEMS / V; ++k) {
-      uint4 r;
-      memcpy(&r, &x[k * V], 16);
-      st_stream_v4(out + my0 + k * V, r);
+    if (!tma_ok) {
+      if (t != NONE) scan_sync_tile_load(in, n, t, bA);
+      if (pending != NONE) scan_sync_tile_load(in, n, pending, bufB);
     }
-  } else {
+    __syncthreads();
+    if (s_has_tma[slot ^ 1]) inflight |= 1u << (slot ^ 1);
+    if (s_has_tma[2]) inflight |= 4u;
+
+    // ---- phase 1 of t: aggregate and publish
+    T agg_t = Op::identity();
+    if (t != NONE) {
+      bool loaded = true;
+      if (inflight & (1u << slot)) {
+        loaded = mbar_wait(&s_bar[slot], parity[slot], spin_limit_ns);
+        if (!loaded) {
+          record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
+          s_abort = 1;
+        } else {
+          parity[slot] ^= 1u;
+          inflight &= ~(1u << slot);
+        }
+      }
+      const uint32_t count = scan_tile_count<T>(n, t);
+      T a = Op::identity();
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i)
-      if (my0 + i < n) out[my0 + i] = x[i];
+      for (int k = 0; k < R; ++k) {
+        const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
+        T x[V];
+        uint4 c = reinterpret_cast<const uint4 *>(bA)[chunk];
+        memcpy(&x[0], &c, 16);
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+          if (chunk * V + j < count) a = op(a, x[j]);
+      }
+      a = warp_reduce(a, op);
+      if (lane == 0) s_wtot[slot][warp] = a;
+      __syncthreads();
+      agg_t = s_wtot[slot][0];
+#pragma unroll
+      for (int i = 1; i < kScanWarps; ++i) agg_t = op(agg_t, s_wtot[slot][i]);
+      if (tid == 0 && loaded && (long long)t != skip_publish_tile) {
+        if (t == 0) st.publish(0u, kStPrefix, op(init, agg_t));
+        else st.publish(t, kStAggregate, agg_t);
+      }
+    }
+
+    // ---- phase 2 of the pending tile p
+    if (pending != NONE) {
+      const unsigned int p = pending;
+      const uint32_t count = scan_tile_count<T>(n, p);
+      if (warp == 0) {
+        T excl = init;
+        bool ok = true;
+        if (p != 0) ok = lookback_exclusive<T>(st, p, op, excl, hdr, spin_limit_ns);
+        if (tid == 0) {
+          if (ok) {
+            if (p != 0 && (long long)p != skip_publish_tile) st.publish(p, kStPrefix, op(excl, pending_agg));
+            s_prefix = excl;
+          } else {
+            s_abort = 1;
+          }
+        }
+      }
+      if (inflight & 4u) {
+        if (!mbar_wait(&s_bar[2], parity[2], spin_limit_ns)) {
+          record_error(hdr, BK_ERR_SPIN_TIMEOUT, p);
+          s_abort = 1;
+        } else {
+          parity[2] ^= 1u;
+          inflight &= ~4u;
+        }
+      }
+      // pass B: rows, offset by the earlier warps' totals (from phase 1)
+      {
+        T carry = Op::identity();
+        bool have = false;
+        for (int i = 0; i < warp; ++i) {
+          carry = have ? op(carry, s_wtot[slot ^ 1][i]) : s_wtot[slot ^ 1][i];
+          have = true;
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
+          T x[V];
+          uint4 c = reinterpret_cast<const uint4 *>(bufB)[chunk];
+          memcpy(&x[0], &c, 16);
+          if (chunk * V + V > count) {
+#pragma unroll
+            for (int j = 0; j < V; ++j)
+              if (chunk * V + j >= count) x[j] = Op::identity();
+          }
+#pragma unroll
+          for (int j = 1; j < V; ++j) x[j] = op(x[j - 1], x[j]);
+          const T incl = warp_inclusive_scan(x[V - 1], op, lane);
+          const T excl = shfl_up(incl, 1);
+          const T row_total = shfl_idx_any(incl, 31);
+          if (lane == 0) {
+            if (have) {
+#pragma unroll
+              for (int j = 0; j < V; ++j) x[j] = op(carry, x[j]);
+            }
+          } else {
+            const T pre = have ? op(carry, excl) : excl;
+#pragma unroll
+            for (int j = 0; j < V; ++j) x[j] = op(pre, x[j]);
+          }
+          memcpy(&c, &x[0], 16);
+          reinterpret_cast<uint4 *>(bufB)[chunk] = c;
+          carry = have ? op(carry, row_total) : row_total;
+          have = true;
+        }
+      }
+      __syncthreads();
+      if (s_abort) break;
+      // pass C: the tile's exclusive prefix
+      const T prefix = s_prefix;
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
+        T x[V];
+        uint4 c = reinterpret_cast<const uint4 *>(bufB)[chunk];
+        memcpy(&x[0], &c, 16);
+#pragma unroll
+        for (int j = 0; j < V; ++j) x[j] = op(prefix, x[j]);
+        memcpy(&c, &x[0], 16);
+        reinterpret_cast<uint4 *>(bufB)[chunk] = c;
+      }
+      const uint64_t base = (uint64_t)p * TILE;
+      if (tma_ok) {
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+          const uint32_t bulk = count & ~(uint32_t)(V - 1);
+          if (bulk > 0) {
+            tma_store_1d_hint(out + base, bufB, bulk * (uint32_t)sizeof(T), stream);
+            tma_store_commit();
+            issued_store = true;
+          }
+          for (uint32_t i = bulk; i < count; ++i) out[base + i] = bufB[i];
+        }
+      } else {
+        __syncthreads();
+        for (uint32_t i = tid; i < count; i += kScanThreads) out[base + i] = bufB[i];
+      }
+    } else if (s_abort) {
+      break;
+    }
+
+    if (t == NONE) break;  // nothing left: the pending tile was the last
+    pending = t;
+    pending_agg = agg_t;
+    __syncthreads();  // bA / s_wtot[slot] reuse and s_ticket visibility
+  }
+
+  // Drain: every bulk store must finish reading shared memory, and on an
+  // abort every prefetch must land, before the CTA's shared memory goes away.
+  if (tid == 0) {
+    if (issued_store) tma_store_wait_all();
+    for (int b = 0; b < 3; ++b)
+      if (inflight & (1u << b)) (void)mbar_wait(&s_bar[b], parity[b], spin_limit_ns);
   }
 }
 
@@ -166,9 +359,17 @@ int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t 
 
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
-  const int vec_ok = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15) == 0;
-  scan_kernel<T, Op><<<(unsigned)tiles, kScanThreads, 0, stream>>>(d_in, d_out, n, init, status, hdr, limit,
-                                                                   dbg.skip_publish_tile, vec_ok);
+  const int tma_ok = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15) == 0;
+  const size_t smem = 3 * (size_t)C::TILE_BYTES;
+  static thread_local bool attr_set = false;  // per host thread; cheap and idempotent
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(scan_kernel<T, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    attr_set = true;
+  }
+  const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * 2);
+  scan_kernel<T, Op><<<grid, kScanThreads, smem, stream>>>(d_in, d_out, n, init, status, hdr, limit,
+                                                           dbg.skip_publish_tile, tma_ok, (unsigned)tiles);
   return host::launch_status();
 }
 

@@ -37,8 +37,8 @@ def test_status_strings_and_version():
 
 def test_workspace_sizes_are_sane_without_a_device():
     ws = bulk_b200.workspace_bytes
-    # scan: 256-byte header + one 8-byte status word per 4096-element tile
-    assert ws("inclusive_scan", "f32", None, 1 << 28) == 256 + (1 << 28) // 4096 * 8
+    # scan: 256-byte header + one 8-byte status word per 8192-element tile
+    assert ws("inclusive_scan", "f32", None, 1 << 28) == 256 + (1 << 28) // 8192 * 8
     assert ws("inclusive_scan", "f64", None, 1 << 28) > ws("inclusive_scan", "f32", None, 1 << 28)
     assert ws("reduce", "f32", None, 1 << 28) >= 256
     assert ws("reduce", "f32", "u32", 10) == 0          # reduce has no payload
