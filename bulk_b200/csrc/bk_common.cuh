@@ -13,7 +13,7 @@
 #include <limits>
 #include <type_traits>
 
-#include "../../include/bulk_b200.h"
+#include "bulk_b200.h"
 
 namespace bk {
 

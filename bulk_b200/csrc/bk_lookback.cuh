@@ -26,7 +26,7 @@
 namespace bk {
 
 enum : unsigned int { kStInvalid = 0u, kStAggregate = 1u, kStPrefix = 2u, kStError = 3u };
-constexpr int kLbPerLane = 4;  // predecessors read per lane per round (128 per warp)
+constexpr int kLbPerLane = 2;  // predecessors read per lane per round (64 per warp)
 
 template <typename P>
 struct TileStatus {
@@ -35,7 +35,7 @@ struct TileStatus {
   unsigned long long *words;
 
   // Rounded up to whole groups of kLbPerLane tiles (the look-back reads groups).
-  __host__ __device__ static size_t bytes(size_t tiles) { return align_up(align_up(tiles, 4) * W * 8, 256); }
+  __host__ __device__ static size_t bytes(size_t tiles) { return align_up(align_up(tiles, (size_t)kLbPerLane) * W * 8, 256); }
   __host__ __device__ static TileStatus at(void *base, size_t /*tiles*/) {
     return TileStatus{reinterpret_cast<unsigned long long *>(base)};
   }
@@ -110,92 +110,95 @@ __device__ __forceinline__ unsigned int wait_status(const Status &st, unsigned i
 // another tile already failed.  All 32 lanes must call it.
 //
 // Lane l reads the aligned group of kLbPerLane tiles g = G - l, where G is the
-// group holding tile - 1: one or more 16-byte vector loads per lane, all issued
-// before any result is used.  Tiles at or after `tile` in the first group do
-// not take part.
+// group holding tile - 1, with 16-byte vector loads issued before any result
+// is used.  Window position q = kLbPerLane * l + j (j = 0 is the lane's
+// nearest tile) orders the window from nearest to farthest.  Only the tiles
+// nearer than the nearest PREFIX are needed, so the warp waits for those alone
+// and never for a slow tile beyond a PREFIX.  Tiles at or after `tile` in the
+// first group do not take part.
 template <typename P, typename Op, typename Status>
 __device__ __forceinline__ bool lookback_exclusive(const Status &st, unsigned int tile, Op op, P &exclusive,
                                                    WsHeader *hdr, unsigned long long limit_ns) {
   constexpr int K = kLbPerLane;
   constexpr int W = Status::W;
-  constexpr int GW = K * W;  // 64-bit words per group (even: K is 4)
+  constexpr int GW = K * W;  // 64-bit words per group
   static_assert(GW % 2 == 0, "group is a whole number of 16-byte vectors");
   const int lane = threadIdx.x & 31;
   long long group = ((long long)tile - 1) / K - lane;
   P acc = Op::identity();
   unsigned long long t0 = 0;
   while (true) {
-    // ---- read the group (tiles 4g .. 4g+3; j = 0 is the nearest = 4g+3)
     P v[K];
     unsigned int f[K];
-    if (group >= 0) {
-      unsigned long long w[GW];
-      const unsigned long long *src = st.words + (size_t)group * GW;
+    int first_p = 32 * K;  // window position of the nearest PREFIX (32K = none)
+    for (unsigned int spins = 0;; ++spins) {
+      // ---- read the group (tiles 4g .. 4g+3; j = 0 is the nearest = 4g+3)
+      if (group >= 0) {
+        unsigned long long w[GW];
+        const unsigned long long *src = st.words + (size_t)group * GW;
 #pragma unroll
-      for (int i = 0; i < GW; i += 2) ld_relaxed_v2_u64(src + i, w[i], w[i + 1]);
+        for (int i = 0; i < GW; i += 2) ld_relaxed_v2_u64(src + i, w[i], w[i + 1]);
 #pragma unroll
-      for (int j = 0; j < K; ++j) {
-        const int t = K - 1 - j;  // position within the group
-        const unsigned int tag = (unsigned int)(w[t * W] >> 32);
-        bool same = true;
-        uint32_t d[W];
+        for (int j = 0; j < K; ++j) {
+          const int t = K - 1 - j;  // position within the group
+          const unsigned int tag = (unsigned int)(w[t * W] >> 32);
+          bool same = true;
+          uint32_t d[W];
 #pragma unroll
-        for (int i = 0; i < W; ++i) {
-          same &= ((unsigned int)(w[t * W + i] >> 32) == tag);
-          d[i] = (uint32_t)(w[t * W + i] & 0xffffffffull);
+          for (int i = 0; i < W; ++i) {
+            same &= ((unsigned int)(w[t * W + i] >> 32) == tag);
+            d[i] = (uint32_t)(w[t * W + i] & 0xffffffffull);
+          }
+          f[j] = same ? tag : kStInvalid;
+          memcpy(&v[j], d, sizeof(P));
         }
-        f[j] = same ? tag : kStInvalid;
-        memcpy(&v[j], d, sizeof(P));
+      } else {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+          f[j] = kStPrefix;  // before tile 0: never chosen, tile 0 always publishes PREFIX
+          v[j] = Op::identity();
+        }
       }
-    } else {
 #pragma unroll
       for (int j = 0; j < K; ++j) {
-        f[j] = kStPrefix;  // before tile 0: never chosen, tile 0 always publishes PREFIX
-        v[j] = Op::identity();
+        if (group * K + (K - 1 - j) >= (long long)tile) {  // at or after this tile
+          f[j] = kStAggregate;
+          v[j] = Op::identity();
+        }
       }
-    }
-    // tiles at or after `tile` (first round, lane 0 only) do not take part
+      // ---- nearest PREFIX, and whether any tile nearer than it is missing
+      int lane_first_p = K, lane_first_inv = K;
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-      const long long idx = group * K + (K - 1 - j);
-      if (idx >= (long long)tile) {
-        f[j] = kStAggregate;
-        v[j] = Op::identity();
+      for (int j = K - 1; j >= 0; --j) {
+        if (f[j] == kStPrefix) lane_first_p = j;
+        if (f[j] == kStInvalid) lane_first_inv = j;
       }
-    }
-    // ---- wait for any not yet valid (nearest first)
-    bool err = false;
-#pragma unroll
-    for (int j = 0; j < K; ++j) {
-      const long long idx = group * K + (K - 1 - j);
-      if (group >= 0 && f[j] == kStInvalid && !err) {
-        f[j] = wait_status(st, (unsigned int)idx, v[j], hdr, limit_ns, t0);
-        err |= (f[j] == kStError);
+      const unsigned int pmask = __ballot_sync(0xffffffffu, lane_first_p < K);
+      first_p = pmask ? (__ffs(pmask) - 1) * K + shfl_idx_any(lane_first_p, __ffs(pmask) - 1) : 32 * K;
+      const bool missing = lane_first_inv < K && (K * lane + lane_first_inv) < first_p;
+      if (!__any_sync(0xffffffffu, missing)) break;
+      // ---- bounded wait
+      if ((spins & 15u) == 15u) {
+        const unsigned long long now = globaltimer_ns();
+        bool give_up = false;
+        if (t0 == 0) t0 = now;
+        else give_up = (now - t0 > limit_ns) || (ld_relaxed_s32(&hdr->status) != 0);
+        if (__any_sync(0xffffffffu, give_up)) {
+          if (lane == 0) record_error(hdr, BK_ERR_SPIN_TIMEOUT, tile);
+          return false;
+        }
       }
+      __nanosleep(spins < 32 ? 32 : 256);
     }
-    if (__any_sync(0xffffffffu, err)) {
-      if (lane == 0) record_error(hdr, BK_ERR_SPIN_TIMEOUT, tile);
-      return false;
-    }
-    // ---- nearest PREFIX: in the lowest lane that has one, at its lowest j
-    int first_j = K;
+    // ---- ordered fold of positions nearer than (and including) first_p
+    P lv = Op::identity();
 #pragma unroll
     for (int j = K - 1; j >= 0; --j)
-      if (f[j] == kStPrefix) first_j = j;
-    const unsigned int pmask = __ballot_sync(0xffffffffu, first_j < K);
-    const int stop_lane = pmask ? (__ffs(pmask) - 1) : 32;
-    // lane-local ordered fold (farthest first), truncated at the PREFIX
-    P lv = Op::identity();
-    if (lane <= stop_lane) {
-      const int last = (lane == stop_lane) ? first_j : K - 1;
-#pragma unroll
-      for (int j = K - 1; j >= 0; --j)
-        if (j <= last) lv = op(lv, v[j]);
-    }
+      if (K * lane + j <= first_p) lv = op(lv, v[j]);
     P wsum = warp_reduce_ordered(lv, op, lane);
     wsum = shfl_idx_any(wsum, 0);
     acc = op(wsum, acc);
-    if (pmask) break;
+    if (first_p < 32 * K) break;
     group -= 32;
   }
   exclusive = acc;

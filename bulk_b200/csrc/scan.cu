@@ -22,8 +22,8 @@
 
 namespace bk {
 
-constexpr int kScanThreads = 256;
-constexpr int kScanWarps = kScanThreads / 32;
+constexpr int kScanWarps = 8;                       // compute warps
+constexpr int kScanThreads = 32 * (kScanWarps + 1);  // + one control warp
 constexpr int kScanRowsPerWarp = 8;
 
 template <typename T>
@@ -55,7 +55,7 @@ template <typename Status>
 __global__ void lookback_init_kernel(Status st, size_t tiles, WsHeader *hdr) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
-  const size_t padded = align_up(tiles, 4);  // whole look-back groups
+  const size_t padded = align_up(tiles, (size_t)kLbPerLane);  // whole look-back groups
   for (size_t t = i; t < padded; t += stride) st.clear(t);
   if (i == 0) hdr->tile_ticket = 0u;
 }
@@ -85,7 +85,7 @@ __device__ __forceinline__ void scan_sync_tile_load(const T *src, uint64_t n, un
   using C = ScanCfg<T>;
   const uint64_t base = (uint64_t)tile * C::TILE;
   const uint32_t count = (uint32_t)((n - base) < (uint64_t)C::TILE ? (n - base) : (uint64_t)C::TILE);
-  for (uint32_t i = threadIdx.x; i < count; i += kScanThreads) buf[i] = src[base + i];
+  for (uint32_t i = threadIdx.x; i < count; i += kScanWarps * 32) buf[i] = src[base + i];
 }
 
 template <typename T>
@@ -94,17 +94,20 @@ __device__ __forceinline__ uint32_t scan_tile_count(uint64_t n, unsigned int til
   return (uint32_t)((n - base) < (uint64_t)ScanCfg<T>::TILE ? (n - base) : (uint64_t)ScanCfg<T>::TILE);
 }
 
-// Persistent two-phase scan.  Each CTA loops over tiles taken from an atomic
-// ticket.  Iteration i of a CTA:
-//   * takes the ticket of its next tile and starts its TMA load (kept in L2
-//     with an evict-last hint) -- one tile ahead;
-//   * starts re-reading its previous tile p from L2 (evict-first);
-//   * phase 1 of the current tile t: reduce it (pass A) and publish its
-//     aggregate (tile 0 publishes its inclusive prefix at once);
-//   * phase 2 of p: warp 0 looks back for p's exclusive prefix -- by now every
-//     predecessor's aggregate is an iteration old, so nothing waits on a slow
-//     load -- while the other warps scan p's rows (pass B); then pass C adds
-//     the prefix and one TMA bulk store writes the tile out (evict-first).
+// Persistent two-phase scan with a control warp.  Each CTA loops over tiles
+// taken from an atomic ticket (the next ticket is always fetched one iteration
+// ahead, so its latency is hidden).  Iteration i of a CTA:
+//   * control warp: starts the TMA load of the next phase-1 tile (kept in L2
+//     with an evict-last hint) and the re-read of the previous tile p from L2
+//     (evict-first);
+//   * compute warps: phase 1 of the current tile t -- reduce it (pass A);
+//   * control warp: publishes t's aggregate (tile 0: its inclusive prefix),
+//     then looks back for p's exclusive prefix -- every predecessor's
+//     aggregate is an iteration old by now, so nothing waits on a slow load --
+//     and publishes p's inclusive prefix;
+//   * compute warps, meanwhile: scan p's rows in registers (pass B); once the
+//     prefix is known they add it and write the tile back to shared memory;
+//   * control warp: one TMA bulk store writes the tile out (evict-first).
 // A tile waiting for its prefix holds no shared memory: its data waits in L2.
 // Every wait points at a lower tile whose ticket a running CTA already took,
 // so the waits always end; each is still bounded by spin_limit_ns.
@@ -129,10 +132,15 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
   __shared__ T s_prefix;
   __shared__ int s_abort;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint64_t keep = l2_policy_evict_last();
-  const uint64_t stream = l2_policy_evict_first();
+  const bool control = (warp == kScanWarps);
+  const bool leader = control && lane == 0;
 
-  if (tid == 0) {
+  unsigned int next_ticket = NONE;  // leader only: ticket for the next phase-1 load
+  bool issued_store = false;        // leader only
+  uint64_t keep = 0, stream = 0;
+  if (leader) {
+    keep = l2_policy_evict_last();
+    stream = l2_policy_evict_first();
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
     mbar_init(&s_bar[2], 1);
@@ -141,15 +149,18 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
     s_has_tma[0] = s_has_tma[1] = s_has_tma[2] = 0;
     const unsigned int t0 = atomicAdd(&hdr->tile_ticket, 1u);
     s_ticket[0] = t0 < num_tiles ? t0 : NONE;
-    if (t0 < num_tiles && tma_ok) s_has_tma[0] = scan_issue_tile_load(in, n, t0, bufA0, &s_bar[0], keep);
+    if (t0 < num_tiles) {
+      if (tma_ok) s_has_tma[0] = scan_issue_tile_load(in, n, t0, bufA0, &s_bar[0], keep);
+      const unsigned int t1 = atomicAdd(&hdr->tile_ticket, 1u);
+      next_ticket = t1 < num_tiles ? t1 : NONE;
+    }
   }
   __syncthreads();
 
   uint32_t parity[3] = {0u, 0u, 0u};
   uint32_t inflight = s_has_tma[0] ? 1u : 0u;  // bit b: a TMA load on s_bar[b] not yet waited for
-  unsigned int pending = NONE;  // tile whose phase 2 is due this iteration
+  unsigned int pending = NONE;                 // tile whose phase 2 is due this iteration
   T pending_agg = Op::identity();
-  bool issued_store = false;
 
   for (int it = 0;; ++it) {
     const int slot = it & 1;
@@ -157,23 +168,24 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
     T *const bA = slot ? bufA1 : bufA0;
     T *const bA_next = slot ? bufA0 : bufA1;
 
-    // ---- start the loads: next phase-1 tile, and the phase-2 re-read
-    if (tid == 0) {
-      unsigned int tn = NONE;
-      if (t != NONE) {
-        const unsigned int x = atomicAdd(&hdr->tile_ticket, 1u);
-        if (x < num_tiles) tn = x;
-      }
-      s_ticket[slot ^ 1] = tn;
-      s_has_tma[slot ^ 1] = 0;
-      if (tn != NONE && tma_ok) s_has_tma[slot ^ 1] = scan_issue_tile_load(in, n, tn, bA_next, &s_bar[slot ^ 1], keep);
+    // ---- control: start the loads (phase-2 re-read first), fetch a ticket
+    if (leader) {
       s_has_tma[2] = 0;
       if (pending != NONE && tma_ok) {
         if (issued_store) tma_store_wait_read();  // bufB free again
         s_has_tma[2] = scan_issue_tile_load(in, n, pending, bufB, &s_bar[2], stream);
       }
+      const unsigned int tn = (t != NONE) ? next_ticket : NONE;
+      s_ticket[slot ^ 1] = tn;
+      s_has_tma[slot ^ 1] = 0;
+      if (tn != NONE && tma_ok) s_has_tma[slot ^ 1] = scan_issue_tile_load(in, n, tn, bA_next, &s_bar[slot ^ 1], keep);
+      next_ticket = NONE;
+      if (tn != NONE) {
+        const unsigned int x = atomicAdd(&hdr->tile_ticket, 1u);  // used next iteration
+        next_ticket = x < num_tiles ? x : NONE;
+      }
     }
-    if (!tma_ok) {
+    if (!tma_ok && !control) {
       if (t != NONE) scan_sync_tile_load(in, n, t, bA);
       if (pending != NONE) scan_sync_tile_load(in, n, pending, bufB);
     }
@@ -181,53 +193,54 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
     if (s_has_tma[slot ^ 1]) inflight |= 1u << (slot ^ 1);
     if (s_has_tma[2]) inflight |= 4u;
 
-    // ---- phase 1 of t: aggregate and publish
-    T agg_t = Op::identity();
+    // ---- compute: phase 1 of t (pass A)
     if (t != NONE) {
-      bool loaded = true;
       if (inflight & (1u << slot)) {
-        loaded = mbar_wait(&s_bar[slot], parity[slot], spin_limit_ns);
-        if (!loaded) {
+        if (!control && !mbar_wait(&s_bar[slot], parity[slot], spin_limit_ns)) {
           record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
           s_abort = 1;
-        } else {
-          parity[slot] ^= 1u;
-          inflight &= ~(1u << slot);
         }
+        parity[slot] ^= 1u;
+        inflight &= ~(1u << slot);
       }
-      const uint32_t count = scan_tile_count<T>(n, t);
-      T a = Op::identity();
+      if (!control) {
+        const uint32_t count = scan_tile_count<T>(n, t);
+        T a = Op::identity();
 #pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
-        T x[V];
-        uint4 c = reinterpret_cast<const uint4 *>(bA)[chunk];
-        memcpy(&x[0], &c, 16);
+        for (int k = 0; k < R; ++k) {
+          const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
+          T x[V];
+          uint4 c = reinterpret_cast<const uint4 *>(bA)[chunk];
+          memcpy(&x[0], &c, 16);
 #pragma unroll
-        for (int j = 0; j < V; ++j)
-          if (chunk * V + j < count) a = op(a, x[j]);
+          for (int j = 0; j < V; ++j)
+            if (chunk * V + j < count) a = op(a, x[j]);
+        }
+        a = warp_reduce(a, op);
+        if (lane == 0) s_wtot[slot][warp] = a;
       }
-      a = warp_reduce(a, op);
-      if (lane == 0) s_wtot[slot][warp] = a;
-      __syncthreads();
+    }
+    __syncthreads();
+    T agg_t = Op::identity();
+    if (t != NONE) {
       agg_t = s_wtot[slot][0];
 #pragma unroll
       for (int i = 1; i < kScanWarps; ++i) agg_t = op(agg_t, s_wtot[slot][i]);
-      if (tid == 0 && loaded && (long long)t != skip_publish_tile) {
+    }
+
+    T y[R][V];
+    if (control) {
+      // ---- publish t's aggregate, look back for p
+      if (leader && t != NONE && !s_abort && (long long)t != skip_publish_tile) {
         if (t == 0) st.publish(0u, kStPrefix, op(init, agg_t));
         else st.publish(t, kStAggregate, agg_t);
       }
-    }
-
-    // ---- phase 2 of the pending tile p
-    if (pending != NONE) {
-      const unsigned int p = pending;
-      const uint32_t count = scan_tile_count<T>(n, p);
-      if (warp == 0) {
+      if (pending != NONE) {
+        const unsigned int p = pending;
         T excl = init;
         bool ok = true;
         if (p != 0) ok = lookback_exclusive<T>(st, p, op, excl, hdr, spin_limit_ns);
-        if (tid == 0) {
+        if (leader) {
           if (ok) {
             if (p != 0 && (long long)p != skip_publish_tile) st.publish(p, kStPrefix, op(excl, pending_agg));
             s_prefix = excl;
@@ -236,75 +249,79 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
           }
         }
       }
+      if (pending != NONE && (inflight & 4u)) {
+        parity[2] ^= 1u;
+        inflight &= ~4u;
+      }
+    } else if (pending != NONE) {
+      // ---- pass B: p's rows in registers, offset by the earlier warps' totals
+      const uint32_t count = scan_tile_count<T>(n, pending);
       if (inflight & 4u) {
         if (!mbar_wait(&s_bar[2], parity[2], spin_limit_ns)) {
-          record_error(hdr, BK_ERR_SPIN_TIMEOUT, p);
+          record_error(hdr, BK_ERR_SPIN_TIMEOUT, pending);
           s_abort = 1;
-        } else {
-          parity[2] ^= 1u;
-          inflight &= ~4u;
         }
+        parity[2] ^= 1u;
+        inflight &= ~4u;
       }
-      // pass B: rows, offset by the earlier warps' totals (from phase 1)
-      {
-        T carry = Op::identity();
-        bool have = false;
-        for (int i = 0; i < warp; ++i) {
-          carry = have ? op(carry, s_wtot[slot ^ 1][i]) : s_wtot[slot ^ 1][i];
-          have = true;
-        }
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
-          T x[V];
-          uint4 c = reinterpret_cast<const uint4 *>(bufB)[chunk];
-          memcpy(&x[0], &c, 16);
-          if (chunk * V + V > count) {
-#pragma unroll
-            for (int j = 0; j < V; ++j)
-              if (chunk * V + j >= count) x[j] = Op::identity();
-          }
-#pragma unroll
-          for (int j = 1; j < V; ++j) x[j] = op(x[j - 1], x[j]);
-          const T incl = warp_inclusive_scan(x[V - 1], op, lane);
-          const T excl = shfl_up(incl, 1);
-          const T row_total = shfl_idx_any(incl, 31);
-          if (lane == 0) {
-            if (have) {
-#pragma unroll
-              for (int j = 0; j < V; ++j) x[j] = op(carry, x[j]);
-            }
-          } else {
-            const T pre = have ? op(carry, excl) : excl;
-#pragma unroll
-            for (int j = 0; j < V; ++j) x[j] = op(pre, x[j]);
-          }
-          memcpy(&c, &x[0], 16);
-          reinterpret_cast<uint4 *>(bufB)[chunk] = c;
-          carry = have ? op(carry, row_total) : row_total;
-          have = true;
-        }
+      T carry = Op::identity();
+      bool have = false;
+      for (int i = 0; i < warp; ++i) {
+        carry = have ? op(carry, s_wtot[slot ^ 1][i]) : s_wtot[slot ^ 1][i];
+        have = true;
       }
-      __syncthreads();
-      if (s_abort) break;
-      // pass C: the tile's exclusive prefix
-      const T prefix = s_prefix;
 #pragma unroll
       for (int k = 0; k < R; ++k) {
         const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
-        T x[V];
         uint4 c = reinterpret_cast<const uint4 *>(bufB)[chunk];
-        memcpy(&x[0], &c, 16);
+        memcpy(&y[k][0], &c, 16);
+        if (chunk * V + V > count) {
 #pragma unroll
-        for (int j = 0; j < V; ++j) x[j] = op(prefix, x[j]);
-        memcpy(&c, &x[0], 16);
-        reinterpret_cast<uint4 *>(bufB)[chunk] = c;
+          for (int j = 0; j < V; ++j)
+            if (chunk * V + j >= count) y[k][j] = Op::identity();
+        }
+#pragma unroll
+        for (int j = 1; j < V; ++j) y[k][j] = op(y[k][j - 1], y[k][j]);
+        const T incl = warp_inclusive_scan(y[k][V - 1], op, lane);
+        const T excl = shfl_up(incl, 1);
+        const T row_total = shfl_idx_any(incl, 31);
+        if (lane == 0) {
+          if (have) {
+#pragma unroll
+            for (int j = 0; j < V; ++j) y[k][j] = op(carry, y[k][j]);
+          }
+        } else {
+          const T pre = have ? op(carry, excl) : excl;
+#pragma unroll
+          for (int j = 0; j < V; ++j) y[k][j] = op(pre, y[k][j]);
+        }
+        carry = have ? op(carry, row_total) : row_total;
+        have = true;
       }
-      const uint64_t base = (uint64_t)p * TILE;
+    }
+    __syncthreads();
+    if (s_abort) break;
+
+    if (pending != NONE) {
+      const uint32_t count = scan_tile_count<T>(n, pending);
+      const uint64_t base = (uint64_t)pending * TILE;
+      if (!control) {
+        // ---- add the tile's exclusive prefix, back to shared memory
+        const T prefix = s_prefix;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
+#pragma unroll
+          for (int j = 0; j < V; ++j) y[k][j] = op(prefix, y[k][j]);
+          uint4 c;
+          memcpy(&c, &y[k][0], 16);
+          reinterpret_cast<uint4 *>(bufB)[chunk] = c;
+        }
+        if (tma_ok) fence_proxy_async_smem();
+      }
+      __syncthreads();
       if (tma_ok) {
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (tid == 0) {
+        if (leader) {
           const uint32_t bulk = count & ~(uint32_t)(V - 1);
           if (bulk > 0) {
             tma_store_1d_hint(out + base, bufB, bulk * (uint32_t)sizeof(T), stream);
@@ -313,23 +330,20 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
           }
           for (uint32_t i = bulk; i < count; ++i) out[base + i] = bufB[i];
         }
-      } else {
-        __syncthreads();
-        for (uint32_t i = tid; i < count; i += kScanThreads) out[base + i] = bufB[i];
+      } else if (!control) {
+        for (uint32_t i = tid; i < count; i += kScanWarps * 32) out[base + i] = bufB[i];
       }
-    } else if (s_abort) {
-      break;
     }
 
     if (t == NONE) break;  // nothing left: the pending tile was the last
     pending = t;
     pending_agg = agg_t;
-    __syncthreads();  // bA / s_wtot[slot] reuse and s_ticket visibility
+    __syncthreads();  // the non-TMA path's plain stores read bufB
   }
 
   // Drain: every bulk store must finish reading shared memory, and on an
   // abort every prefetch must land, before the CTA's shared memory goes away.
-  if (tid == 0) {
+  if (leader) {
     if (issued_store) tma_store_wait_all();
     for (int b = 0; b < 3; ++b)
       if (inflight & (1u << b)) (void)mbar_wait(&s_bar[b], parity[b], spin_limit_ns);
