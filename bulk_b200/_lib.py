@@ -71,7 +71,7 @@ class BulkError(RuntimeError):
 def _load():
     if not LIB_PATH.exists():
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m bulk_b200.build` "
+            f"{LIB_PATH} is missing: build it with `python bulk_b200/build.py` "
             "(the CUDA library is the only implementation; there is no fallback)")
     lib = ctypes.CDLL(str(LIB_PATH))
     for name, (res, args) in DECLS.items():

@@ -5,7 +5,8 @@ Each ``csrc/*.cu`` file is compiled separately (in parallel) with
 linked into ``bulk_b200/lib/libbulkb200.so`` against the static CUDA runtime,
 so the library carries no dependency on a particular libcudart.so.
 
-Usage: ``python -m bulk_b200.build [--force] [--verbose]``.
+Usage: ``python bulk_b200/build.py [--force] [--verbose]`` (run it as a script: importing
+the package loads the library it builds).
 """
 from __future__ import annotations
 

@@ -19,8 +19,11 @@ if str(ROOT) not in sys.path:
 # container); on a GPU machine the prebuilt library is used as shipped.
 _lib = ROOT / "bulk_b200" / "lib" / "libbulkb200.so"
 if not _lib.exists() and shutil.which("nvcc"):
-    from bulk_b200.build import build as _build
-    _build()
+    import importlib.util
+    _spec = importlib.util.spec_from_file_location("bulk_b200_build_script", ROOT / "bulk_b200" / "build.py")
+    _mod = importlib.util.module_from_spec(_spec)
+    _spec.loader.exec_module(_mod)
+    _mod.build()
 
 
 def pytest_configure(config):
