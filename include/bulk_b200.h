@@ -136,6 +136,17 @@ BK_API int bk_inclusive_scan_max_u64(const uint64_t *d_in, uint64_t n, uint64_t 
 BK_API int bk_inclusive_scan_max_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_inclusive_scan_max_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
+/* Allocation-free variant of bk_inclusive_scan_sum_f32 (no counterpart in the
+ * reference).  For callers that cannot allocate device memory: the scan's
+ * scratch lives in a fixed 1 MiB + 256-byte array inside the library's own
+ * device memory, held by every GPU that loads the library until exit.
+ * n is limited to 2^30 elements (BK_ERR_TOO_LARGE beyond).  The first call on
+ * a device looks up the array's device address; make that call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (concurrent streams, other threads) race and corrupt each other, so
+ * serialise them.  Device-side wait errors are not reported by this variant. */
+BK_API int bk_inclusive_scan_sum_f32_noalloc(const float *d_in, uint64_t n, float init, float *d_out, bk_stream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
