@@ -9,7 +9,9 @@ from .algorithms import (  # noqa: F401
     debug_set_fault,
     dtype_tag,
     inclusive_scan,
+    merge,
     reduce,
+    stable_sort_by_key,
     workspace_bytes,
     workspace_status,
     workspaces,

@@ -160,3 +160,59 @@ def inclusive_scan(x: torch.Tensor, init=0, op: str = "sum", out: torch.Tensor |
     fn = getattr(lib, f"bk_inclusive_scan_{op}_{tag}")
     check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
     return out
+
+
+def _payload_tag(t: torch.Tensor | None) -> str | None:
+    if t is None:
+        return None
+    if t.element_size() == 4:
+        return "u32"
+    if t.element_size() == 8:
+        return "u64"
+    raise TypeError("payloads must be 4- or 8-byte elements")
+
+
+def merge(a: torch.Tensor, b: torch.Tensor, a_vals: torch.Tensor | None = None, b_vals: torch.Tensor | None = None,
+          out: torch.Tensor | None = None, out_vals: torch.Tensor | None = None,
+          stream: torch.cuda.Stream | None = None):
+    """Stable merge of sorted a and b (ties: a first).  Returns keys, or (keys, vals) with payloads."""
+    dev = _require_cuda(a, b, a_vals, b_vals, out, out_vals)
+    if a.dtype != b.dtype:
+        raise TypeError("a and b must have the same dtype")
+    tag = dtype_tag(a.dtype)
+    n = a.numel() + b.numel()
+    if out is None:
+        out = torch.empty(n, dtype=a.dtype, device=dev)
+    s = _stream_handle(stream, dev)
+    ws, wsb = _ws("merge", tag, _payload_tag(a_vals), n, dev, s)
+    if a_vals is None:
+        fn = getattr(lib, f"bk_merge_{tag}")
+        check(fn(_ptr(a), a.numel(), _ptr(b), b.numel(), _ptr(out), ws, wsb, s), fn.__name__)
+        return out
+    if b_vals is None or a_vals.element_size() != b_vals.element_size():
+        raise TypeError("a_vals and b_vals must both be given, with the same element size")
+    if out_vals is None:
+        out_vals = torch.empty(n, dtype=a_vals.dtype, device=dev)
+    fn = getattr(lib, f"bk_merge_by_key_{tag}_{_payload_tag(a_vals)}")
+    check(fn(_ptr(a), _ptr(a_vals), a.numel(), _ptr(b), _ptr(b_vals), b.numel(), _ptr(out), _ptr(out_vals),
+             ws, wsb, s), fn.__name__)
+    return out, out_vals
+
+
+def stable_sort_by_key(keys: torch.Tensor, vals: torch.Tensor | None = None,
+                       stream: torch.cuda.Stream | None = None):
+    """In-place stable sort of keys (and vals with them).  Returns keys, or (keys, vals)."""
+    dev = _require_cuda(keys, vals)
+    tag = dtype_tag(keys.dtype)
+    n = keys.numel()
+    if vals is not None and vals.numel() != n:
+        raise ValueError("keys and vals must have the same length")
+    s = _stream_handle(stream, dev)
+    ws, wsb = _ws("sort_by_key", tag, _payload_tag(vals), n, dev, s)
+    if vals is None:
+        fn = getattr(lib, f"bk_sort_keys_{tag}")
+        check(fn(_ptr(keys), n, ws, wsb, s), fn.__name__)
+        return keys
+    fn = getattr(lib, f"bk_sort_by_key_{tag}_{_payload_tag(vals)}")
+    check(fn(_ptr(keys), _ptr(vals), n, ws, wsb, s), fn.__name__)
+    return keys, vals

@@ -1,6 +1,4 @@
 #include "bk_common.cuh"
 namespace bk {
-size_t merge_workspace_bytes(int, int, uint64_t) { return 0; }
-size_t sort_workspace_bytes(int, int, uint64_t) { return 0; }
 size_t rbk_workspace_bytes(int, int, uint64_t) { return 0; }
 }

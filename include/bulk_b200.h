@@ -136,6 +136,60 @@ BK_API int bk_inclusive_scan_max_u64(const uint64_t *d_in, uint64_t n, uint64_t 
 BK_API int bk_inclusive_scan_max_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_inclusive_scan_max_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
+
+/* ---- merge ----------------------------------------------------------------
+ * Stable merge of two sorted ranges under operator<: equal keys keep A before
+ * B and each input's own order (merge_path, bulk/algorithm/merge.hpp:35-60,
+ * and the serial merge, merge.hpp:63-170).  out has na + nb elements.
+ * bk_merge_* replaces my_merge(first1, last1, first2, last2, result, comp),
+ * merge.cu:127-162 (keys only); bk_merge_by_key_* adds a 4- or 8-byte payload
+ * moved with each key, as the bounded group merge_by_key does,
+ * bulk/algorithm/merge.hpp:507-607.  Keys must not be NaN. */
+BK_API int bk_merge_i32(const int32_t *a, uint64_t na, const int32_t *b, uint64_t nb, int32_t *out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_u32(const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb, uint32_t *out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_i64(const int64_t *a, uint64_t na, const int64_t *b, uint64_t nb, int64_t *out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_u64(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, uint64_t *out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_f32(const float *a, uint64_t na, const float *b, uint64_t nb, float *out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_f64(const double *a, uint64_t na, const double *b, uint64_t nb, double *out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_i32_u32(const int32_t *a_keys, const uint32_t *a_vals, uint64_t na, const int32_t *b_keys, const uint32_t *b_vals, uint64_t nb, int32_t *out_keys, uint32_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_i32_u64(const int32_t *a_keys, const uint64_t *a_vals, uint64_t na, const int32_t *b_keys, const uint64_t *b_vals, uint64_t nb, int32_t *out_keys, uint64_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_u32_u32(const uint32_t *a_keys, const uint32_t *a_vals, uint64_t na, const uint32_t *b_keys, const uint32_t *b_vals, uint64_t nb, uint32_t *out_keys, uint32_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_u32_u64(const uint32_t *a_keys, const uint64_t *a_vals, uint64_t na, const uint32_t *b_keys, const uint64_t *b_vals, uint64_t nb, uint32_t *out_keys, uint64_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_i64_u32(const int64_t *a_keys, const uint32_t *a_vals, uint64_t na, const int64_t *b_keys, const uint32_t *b_vals, uint64_t nb, int64_t *out_keys, uint32_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_i64_u64(const int64_t *a_keys, const uint64_t *a_vals, uint64_t na, const int64_t *b_keys, const uint64_t *b_vals, uint64_t nb, int64_t *out_keys, uint64_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_u64_u32(const uint64_t *a_keys, const uint32_t *a_vals, uint64_t na, const uint64_t *b_keys, const uint32_t *b_vals, uint64_t nb, uint64_t *out_keys, uint32_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_u64_u64(const uint64_t *a_keys, const uint64_t *a_vals, uint64_t na, const uint64_t *b_keys, const uint64_t *b_vals, uint64_t nb, uint64_t *out_keys, uint64_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_f32_u32(const float *a_keys, const uint32_t *a_vals, uint64_t na, const float *b_keys, const uint32_t *b_vals, uint64_t nb, float *out_keys, uint32_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_f32_u64(const float *a_keys, const uint64_t *a_vals, uint64_t na, const float *b_keys, const uint64_t *b_vals, uint64_t nb, float *out_keys, uint64_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_f64_u32(const double *a_keys, const uint32_t *a_vals, uint64_t na, const double *b_keys, const uint32_t *b_vals, uint64_t nb, double *out_keys, uint32_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_merge_by_key_f64_u64(const double *a_keys, const uint64_t *a_vals, uint64_t na, const double *b_keys, const uint64_t *b_vals, uint64_t nb, double *out_keys, uint64_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
+/* ---- stable sort by key (merge sort) --------------------------------------
+ * In-place stable sort of keys[0..n) under operator<, moving vals with their
+ * keys; equal keys keep their input order.  Replaces
+ * stable_merge_sort_by_key(keys_first, keys_last, values_first, comp),
+ * merge_sort_by_key.cu:150-209 (block sort bulk/algorithm/sort.hpp:152-166,
+ * stable_merge_sort.hpp:125-206, then merge-path passes).  Keys must not be
+ * NaN.  bk_sort_keys_* sorts keys alone. */
+BK_API int bk_sort_keys_i32(int32_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_keys_u32(uint32_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_keys_i64(int64_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_keys_u64(uint64_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_keys_f32(float *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_keys_f64(double *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i32_u32(int32_t *keys, uint32_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i32_u64(int32_t *keys, uint64_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u32_u32(uint32_t *keys, uint32_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u32_u64(uint32_t *keys, uint64_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i64_u32(int64_t *keys, uint32_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i64_u64(int64_t *keys, uint64_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u64_u64(uint64_t *keys, uint64_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f32_u32(float *keys, uint32_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f32_u64(float *keys, uint64_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f64_u32(double *keys, uint32_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f64_u64(double *keys, uint64_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
 /* Allocation-free variant of bk_inclusive_scan_sum_f32 (no counterpart in the
  * reference).  For callers that cannot allocate device memory: the scan's
  * scratch lives in a fixed 1 MiB + 256-byte array inside the library's own

@@ -1,0 +1,100 @@
+"""GPU parity of bk_sort_by_key_* / bk_sort_keys_* (stable merge sort) against
+the oracle: keys and payload order bit-exact."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import bulk_b200
+import oracle
+from tests.gpu_util import NP, dev, gen, host
+from tests.sizes import reference_sizes
+
+pytestmark = pytest.mark.gpu
+KEYS = ["i32", "u32", "i64", "u64", "f32", "f64"]
+
+
+def test_known_answer_hash_fill(cuda):
+    # merge_sort_by_key.cu:315-380: keys and values hash-filled, the drivers' size schedule,
+    # compared with a stable sort_by_key
+    for n in reference_sizes():
+        keys = oracle.ref_hash_fill_i32(n)
+        vals = keys.copy()
+        gk, gv = bulk_b200.stable_sort_by_key(dev(keys), dev(vals))
+        order = np.argsort(keys, kind="stable")
+        assert np.array_equal(host(gk), keys[order]), n
+        assert np.array_equal(host(gv), vals[order]), n
+
+
+def _keys(tag, n, seed, coarse):
+    x = gen(tag, n, seed)
+    if coarse:  # many duplicates: stability matters
+        if tag in ("f32", "f64"):
+            x = np.floor(x * 50).astype(x.dtype)
+        else:
+            x = (x // np.array(1 << 20 if tag in ("i32", "u32") else 1 << 52).astype(x.dtype)).astype(x.dtype)
+    return x
+
+
+@pytest.mark.parametrize("tag", KEYS)
+@pytest.mark.parametrize("payload", [None, np.uint32, np.uint64])
+def test_edge_sizes(cuda, tag, payload):
+    sizes = [0, 1, 2, 3, 17, 1023, 4096, 8191, 8192, 8193, 16385, 3 * 8192 + 5, 100003]
+    for i, n in enumerate(sizes):
+        for coarse in (False, True):
+            keys = _keys(tag, n, 300 + i, coarse)
+            if payload is None:
+                got = host(bulk_b200.stable_sort_by_key(dev(keys)))
+                assert np.array_equal(got, np.sort(keys, kind="stable")), (tag, n)
+            else:
+                vals = np.arange(n, dtype=payload)
+                gk, gv = bulk_b200.stable_sort_by_key(dev(keys), dev(vals))
+                wk, wv = oracle.stable_sort_by_key(keys, vals)
+                assert np.array_equal(host(gk), wk) and np.array_equal(host(gv), wv), (tag, n, coarse)
+
+
+def test_presorted_reversed_and_constant(cuda):
+    n = 70001
+    for keys in (np.arange(n, dtype=np.int32), np.arange(n, 0, -1).astype(np.int32), np.zeros(n, np.int32)):
+        vals = np.arange(n, dtype=np.uint32)
+        gk, gv = bulk_b200.stable_sort_by_key(dev(keys), dev(vals))
+        order = np.argsort(keys, kind="stable")
+        assert np.array_equal(host(gv), order.astype(np.uint32))
+
+
+def test_max_key_values_are_not_confused_with_padding(cuda):
+    # partial tiles are padded with the largest key; real largest keys must stay ahead of it
+    n = 8192 + 37
+    keys = np.full(n, 0xFFFFFFFF, dtype=np.uint32)
+    keys[::3] = 5
+    vals = np.arange(n, dtype=np.uint32)
+    gk, gv = bulk_b200.stable_sort_by_key(dev(keys), dev(vals))
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(host(gk), keys[order]) and np.array_equal(host(gv), order.astype(np.uint32))
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("tag", ["u32", "u64"])
+def test_full_size_2_26_payload_is_index(cuda, tag):
+    """The benchmark configuration: 2^26 keys over the full range, payload =
+    original index.  Properties: keys nondecreasing, equal keys keep increasing
+    payloads (stability), payload is a permutation, keys[i] == input[payload[i]]."""
+    n = 1 << 26
+    keys0 = dev(gen(tag, n, 3 if tag == "u32" else 4))
+    keys = keys0.clone()
+    vals = torch.arange(n, dtype=torch.int32, device=cuda)
+    bulk_b200.stable_sort_by_key(keys, vals)
+    # compare as signed views (unsigned order = signed order with the sign bit flipped)
+    if tag == "u32":
+        k = keys.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+        k0 = keys0.view(torch.int32)
+        ks = keys.view(torch.int32)
+    else:
+        k = keys.view(torch.int64) ^ torch.tensor(-(1 << 63), dtype=torch.int64, device=cuda)
+        k0 = keys0.view(torch.int64)
+        ks = keys.view(torch.int64)
+    ok = (k[1:] > k[:-1]) | ((k[1:] == k[:-1]) & (vals[1:] > vals[:-1]))
+    assert bool(ok.all())
+    assert torch.equal(torch.sort(vals).values, torch.arange(n, dtype=torch.int32, device=cuda))
+    assert torch.equal(ks, k0[vals.long()])
