@@ -11,6 +11,7 @@ from .algorithms import (  # noqa: F401
     inclusive_scan,
     merge,
     reduce,
+    reduce_by_key,
     stable_sort_by_key,
     workspace_bytes,
     workspace_status,

@@ -216,3 +216,34 @@ def stable_sort_by_key(keys: torch.Tensor, vals: torch.Tensor | None = None,
     fn = getattr(lib, f"bk_sort_by_key_{tag}_{_payload_tag(vals)}")
     check(fn(_ptr(keys), _ptr(vals), n, ws, wsb, s), fn.__name__)
     return keys, vals
+
+
+def reduce_by_key(keys: torch.Tensor, vals: torch.Tensor, out_keys: torch.Tensor | None = None,
+                  out_vals: torch.Tensor | None = None, num_out: torch.Tensor | None = None,
+                  stream: torch.cuda.Stream | None = None, sync: bool = True):
+    """One (key, sum) pair per run of equal consecutive keys.
+
+    Returns (out_keys, out_vals, count).  With ``sync=True`` (the reference's
+    behaviour, reduce_by_key.cu:269) count is a Python int and the outputs are
+    trimmed to it; with ``sync=False`` count stays a 1-element device tensor
+    and the outputs are the full-length buffers.
+    """
+    dev = _require_cuda(keys, vals, out_keys, out_vals, num_out)
+    n = keys.numel()
+    if vals.numel() != n:
+        raise ValueError("keys and vals must have the same length")
+    kt, vt = dtype_tag(keys.dtype), dtype_tag(vals.dtype)
+    if out_keys is None:
+        out_keys = torch.empty(max(n, 1), dtype=keys.dtype, device=dev)
+    if out_vals is None:
+        out_vals = torch.empty(max(n, 1), dtype=vals.dtype, device=dev)
+    if num_out is None:
+        num_out = torch.empty(1, dtype=torch.int64, device=dev)
+    s = _stream_handle(stream, dev)
+    ws, wsb = _ws("reduce_by_key", kt, vt, n, dev, s)
+    fn = getattr(lib, f"bk_reduce_by_key_{kt}_{vt}")
+    check(fn(_ptr(keys), _ptr(vals), n, _ptr(out_keys), _ptr(out_vals), _ptr(num_out), ws, wsb, s), fn.__name__)
+    if not sync:
+        return out_keys, out_vals, num_out
+    c = int(num_out.item())
+    return out_keys[:c], out_vals[:c], c

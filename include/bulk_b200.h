@@ -190,6 +190,28 @@ BK_API int bk_sort_by_key_f32_u64(float *keys, uint64_t *vals, uint64_t n, void 
 BK_API int bk_sort_by_key_f64_u32(double *keys, uint32_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_sort_by_key_f64_u64(double *keys, uint64_t *vals, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
+
+/* ---- reduce_by_key (pred = equal_to, op = plus) -----------------------------
+ * One output pair per maximal run of equal consecutive keys, in run order:
+ * out_keys[r] = the run's key, out_vals[r] = the sum of its values, and
+ * *d_num_out = the number of runs (written on the device; n == 0 writes 0).
+ * out_keys / out_vals need room for n elements in the worst case.  Integer
+ * sums wrap.  n < 2^32.  Replaces my_reduce_by_key(keys_first, keys_last,
+ * values_first, keys_result, values_result, pred, binary_op),
+ * reduce_by_key.cu:176-272 (bulk::reduce_by_key,
+ * bulk/algorithm/reduce_by_key.hpp:115-216), whose result size the reference
+ * returns through a synchronous device-to-host copy (:269). */
+BK_API int bk_reduce_by_key_i32_i32(const int32_t *keys, const int32_t *vals, uint64_t n, int32_t *out_keys, int32_t *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i32_i64(const int32_t *keys, const int64_t *vals, uint64_t n, int32_t *out_keys, int64_t *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i32_f32(const int32_t *keys, const float *vals, uint64_t n, int32_t *out_keys, float *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i32_f64(const int32_t *keys, const double *vals, uint64_t n, int32_t *out_keys, double *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_u32_f32(const uint32_t *keys, const float *vals, uint64_t n, uint32_t *out_keys, float *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_u32_f64(const uint32_t *keys, const double *vals, uint64_t n, uint32_t *out_keys, double *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i64_i32(const int64_t *keys, const int32_t *vals, uint64_t n, int64_t *out_keys, int32_t *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i64_i64(const int64_t *keys, const int64_t *vals, uint64_t n, int64_t *out_keys, int64_t *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i64_f32(const int64_t *keys, const float *vals, uint64_t n, int64_t *out_keys, float *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i64_f64(const int64_t *keys, const double *vals, uint64_t n, int64_t *out_keys, double *out_vals, uint64_t *d_num_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
 /* Allocation-free variant of bk_inclusive_scan_sum_f32 (no counterpart in the
  * reference).  For callers that cannot allocate device memory: the scan's
  * scratch lives in a fixed 1 MiB + 256-byte array inside the library's own
