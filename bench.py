@@ -12,8 +12,10 @@ value  = algorithmic bytes per step (reduce N*s, scan 2*N*s) / device time,
 e2e    = the same through the C-ABI with host buffers: pinned-host -> device
          copies of the step's inputs and device -> host copies of every result
          inside the timed region.
-ops    = per-op GB/s at the other benchmark configurations (merge_by_key,
-         stable sort_by_key, reduce_by_key), timed after the headline.
+ops    = per-op GB/s: the headline's six calls, and the other benchmark
+         configurations (merge_by_key 2 x 2^26 f32/u32, stable sort_by_key
+         2^26 u32/u64 keys with u32 payload, reduce_by_key 2^27 i32 keys with
+         geometric / Zipf runs and f32 / f64 values), timed after the headline.
 
 ``--impl reference`` times the reference's CPU implementation of the same
 reduce + scan on the host cores instead (rank 0 only).
@@ -266,6 +268,144 @@ def e2e(args, device, xs):
     return a.elapsed_time(b) / steps, h2d, d2h, steps
 
 
+def _time_op(fn, prep=None, reps=5, warm=2):
+    """Mean device time (ms) of fn() over reps, CUDA events on the current
+    stream; prep() (untimed) runs before each call."""
+    import torch
+    stream = torch.cuda.current_stream()
+    for _ in range(warm):
+        if prep:
+            prep()
+        fn()
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(reps):
+        if prep:
+            prep()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    return tot / reps
+
+
+def _geometric_runs(n, mean, g, device):
+    """i32 run-index keys with run lengths 1 + Geometric(1/mean), truncated to n elements."""
+    import torch
+    p = 1.0 / mean
+    m = int(n / mean * 1.1) + 1024
+    while True:
+        u = torch.rand(m, generator=g, device=device, dtype=torch.float64)
+        lens = 1 + torch.floor(torch.log1p(-u) / math.log1p(-p)).to(torch.int64)
+        if int(lens.sum()) >= n:
+            break
+        m *= 2
+    keys = torch.repeat_interleave(torch.arange(m, device=device, dtype=torch.int32), lens)
+    return keys[:n].contiguous()
+
+
+def _zipf_runs(n, s_exp, cap, g, device):
+    """i32 run-index keys whose run lengths are Zipf(s_exp)-like (a bounded
+    Pareto draw, rounded down) capped at cap, truncated to n elements."""
+    import torch
+    a = 1.0 - s_exp
+    top = (cap + 1.0) ** a - 1.0
+    m = max(1024, n // 64)
+    while True:
+        u = torch.rand(m, generator=g, device=device, dtype=torch.float64)
+        lens = torch.floor((1.0 + u * top) ** (1.0 / a)).clamp(1, cap).to(torch.int64)
+        csum = torch.cumsum(lens, 0)
+        if int(csum[-1]) >= n:
+            break
+        m *= 2
+    r = int(torch.searchsorted(csum, torch.tensor([n], device=device, dtype=torch.int64)).item()) + 1
+    lens = lens[:r].clone()
+    lens[-1] -= int(csum[r - 1]) - n
+    keys = torch.repeat_interleave(torch.arange(r, device=device, dtype=torch.int32), lens)
+    return keys
+
+
+def other_ops(device, peak, quick=False, shift=0):
+    """Per-op effective GB/s at the other benchmark configurations (sizes / 2^shift)."""
+    import torch
+
+    import bulk_b200
+    g = torch.Generator(device=device)
+    g.manual_seed(1)
+    res = {}
+    reps = 3 if quick else 5
+
+    # merge_by_key: A, B = 2^26 float32 U[0,1) each (~1% cross duplicates), u32 payloads
+    n = 1 << (26 - shift)
+    a = torch.sort(torch.rand(n, generator=g, device=device)).values
+    b = torch.rand(n, generator=g, device=device)
+    idx = torch.randint(0, n, (n // 100,), generator=g, device=device)
+    b[idx] = a[torch.randint(0, n, (n // 100,), generator=g, device=device)]
+    b = torch.sort(b).values
+    av = torch.arange(n, dtype=torch.int32, device=device)
+    bv = av + n
+    ok = torch.empty(2 * n, dtype=torch.float32, device=device)
+    ov = torch.empty(2 * n, dtype=torch.int32, device=device)
+    ms = _time_op(lambda: bulk_b200.merge(a, b, av, bv, out=ok, out_vals=ov), reps=reps)
+    byts = 2 * (2 * n) * 8
+    res[f"merge_by_key_f32_u32_2x2^{26 - shift}"] = {"ms": ms, "GBps": byts / ms / 1e6, "frac_of_hbm": byts / ms / 1e6 / peak,
+                                          "algorithmic_bytes": byts}
+    del a, b, av, bv, ok, ov
+
+    # stable sort_by_key: 2^26 u32 keys (full range) / 2^26 u64 keys, payload = index
+    for tag in ("u32", "u64"):
+        if tag == "u32":
+            k0 = torch.randint(-(1 << 31), (1 << 31) - 1, (n,), generator=g, device=device,
+                               dtype=torch.int32).view(torch.uint32)
+        else:
+            hi = torch.randint(-(1 << 31), (1 << 31) - 1, (n,), generator=g, device=device, dtype=torch.int32)
+            lo = torch.randint(-(1 << 31), (1 << 31) - 1, (n,), generator=g, device=device, dtype=torch.int32)
+            k0 = ((hi.to(torch.int64) << 32) | (lo.to(torch.int64) & 0xFFFFFFFF)).view(torch.uint64)
+            del hi, lo
+        v0 = torch.arange(n, dtype=torch.int32, device=device)
+        k, v = k0.clone(), v0.clone()
+
+        def prep():
+            k.copy_(k0)
+            v.copy_(v0)
+        ms = _time_op(lambda: bulk_b200.stable_sort_by_key(k, v), prep=prep, reps=reps)
+        byts = 2 * n * (k0.element_size() + 4)
+        passes = 0
+        w = 8192 if tag == "u32" else 4096
+        while w < n:
+            w *= 2
+            passes += 1
+        res[f"sort_by_key_{tag}_u32_2^{26 - shift}"] = {
+            "ms": ms, "GBps": byts / ms / 1e6, "frac_of_hbm": byts / ms / 1e6 / peak, "algorithmic_bytes": byts,
+            "merge_passes": passes,
+            "bytes_moved_by_design": (passes + 1) * byts,
+            "GBps_of_bytes_moved": (passes + 1) * byts / ms / 1e6}
+        del k0, v0, k, v
+
+    # reduce_by_key: 2^27 pairs, i32 keys in runs (geometric mean 16 / Zipf 1.2 cap 2^20), f32/f64 U[0,1)
+    n = 1 << (27 - shift)
+    for kind in ("geometric", "zipf"):
+        keys = _geometric_runs(n, 16.0, g, device) if kind == "geometric" else _zipf_runs(n, 1.2, 1 << 20, g, device)
+        for vt, dt in (("f32", torch.float32), ("f64", torch.float64)):
+            vals = torch.rand(n, generator=g, device=device, dtype=dt)
+            ok = torch.empty(n, dtype=torch.int32, device=device)
+            ov = torch.empty(n, dtype=dt, device=device)
+            cnt = torch.empty(1, dtype=torch.int64, device=device)
+            ms = _time_op(lambda: bulk_b200.reduce_by_key(keys, vals, ok, ov, cnt, sync=False), reps=reps)
+            u = int(cnt.item())
+            sv = vals.element_size()
+            byts = n * (4 + sv) + u * (4 + sv) + 8
+            res[f"reduce_by_key_i32_{vt}_{kind}_2^{27 - shift}"] = {"ms": ms, "GBps": byts / ms / 1e6,
+                                                          "frac_of_hbm": byts / ms / 1e6 / peak,
+                                                          "algorithmic_bytes": byts, "runs": u}
+            del vals, ok, ov, cnt
+        del keys
+    torch.cuda.empty_cache()
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -275,6 +415,8 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=N_HEADLINE, help=argparse.SUPPRESS)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-ops", action="store_true")
+    ap.add_argument("--ops-shift", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -315,6 +457,8 @@ def main(argv=None):
     e2e_ms, h2d, d2h, e2e_steps = e2e(args, device, xs)
     del xs
     torch.cuda.empty_cache()
+    if not args.no_other_ops:
+        ops.update(other_ops(device, peak, shift=args.ops_shift))
 
     line = None
     if rank == 0:

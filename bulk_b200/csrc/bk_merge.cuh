@@ -46,9 +46,23 @@ __host__ __device__ constexpr K key_max() {
   return std::numeric_limits<K>::has_infinity ? std::numeric_limits<K>::infinity() : std::numeric_limits<K>::max();
 }
 
+// Shared-memory layout with one pad element after every 32: a thread reading
+// or writing its own ITEMS consecutive elements (stride ITEMS between lanes)
+// and a warp reading 32 consecutive elements both hit 32 distinct banks.
+__host__ __device__ constexpr int pad32(int i) { return i + (i >> 5); }
+__host__ __device__ constexpr int padded_len(int n) { return n + (n >> 5) + 1; }
+
+// A view of a padded shared-memory array starting at unpadded index `off`.
+template <typename K>
+struct PView {
+  const K *base;
+  int off;
+  __device__ __forceinline__ K operator[](int i) const { return base[pad32(off + i)]; }
+};
+
 // merge_path over global or shared memory (64-bit or 32-bit indices).
-template <typename K, typename I>
-__device__ __forceinline__ I merge_path(const K *a, I na, const K *b, I nb, I diag) {
+template <typename K, typename I, typename A, typename B>
+__device__ __forceinline__ I merge_path(A a, I na, B b, I nb, I diag) {
   I lo = diag > nb ? diag - nb : I(0);
   I hi = diag < na ? diag : na;
   while (lo < hi) {
@@ -60,10 +74,10 @@ __device__ __forceinline__ I merge_path(const K *a, I na, const K *b, I nb, I di
 }
 
 // Serial stable merge of ITEMS outputs from shared memory: A = s[ia..na),
-// B = s[nb0 + ib .. nb0 + nb) (B stored right after A at offset nb0 = na).
-// Writes keys and the shared-memory source index of each output.
-template <int ITEMS, typename K>
-__device__ __forceinline__ void serial_merge(const K *s, int na, int nb, int ia, int ib, K (&keys)[ITEMS],
+// B = s[na + ib .. na + nb) (B stored right after A).  Writes keys and the
+// (unpadded) index of each output's source.  S indexes like an array.
+template <int ITEMS, typename K, typename S>
+__device__ __forceinline__ void serial_merge(S s, int na, int nb, int ia, int ib, K (&keys)[ITEMS],
                                              int (&src)[ITEMS], int valid) {
   K ka = ia < na ? s[ia] : K();
   K kb = ib < nb ? s[na + ib] : K();
@@ -109,30 +123,68 @@ __device__ __forceinline__ void stage_out(T *g, const T *s, int n) {
   }
 }
 
+// Coalesced copy of n elements from a padded shared-memory array to global
+// memory: each thread gathers 16 bytes (conflict-free) and stores them as one
+// vector when the destination is 16-byte aligned.
+template <int THREADS, typename T>
+__device__ __forceinline__ void stage_out_padded(T *g, const T *s, int n) {
+  constexpr int VE = 16 / (int)sizeof(T);
+  if ((reinterpret_cast<uintptr_t>(g) & 15) == 0) {
+    const int nv = n / VE;
+    for (int c = threadIdx.x; c < nv; c += THREADS) {
+      T v[VE];
+#pragma unroll
+      for (int j = 0; j < VE; ++j) v[j] = s[pad32(c * VE + j)];
+      uint4 q;
+      memcpy(&q, v, 16);
+      reinterpret_cast<uint4 *>(g)[c] = q;
+    }
+    for (int i = nv * VE + threadIdx.x; i < n; i += THREADS) g[i] = s[pad32(i)];
+  } else {
+    for (int i = threadIdx.x; i < n; i += THREADS) g[i] = s[pad32(i)];
+  }
+}
+
 // One merge tile.  The caller supplies the tile's A and B ranges (global
 // pointers and lengths, la + lb <= THREADS * ITEMS) and the output position.
-// Shared memory: THREADS * ITEMS keys, then THREADS * ITEMS payloads.
+// Shared memory (padded layout): padded_len(THREADS * ITEMS) keys, then as
+// many payloads.
 template <int THREADS, int ITEMS, typename K, typename P>
 __device__ __forceinline__ void merge_tile(const K *ak, const P *av, int la, const K *bk, const P *bv, int lb, K *ok,
                                            P *ov, unsigned char *smem) {
   constexpr int T = THREADS * ITEMS;
   K *sk = reinterpret_cast<K *>(smem);
   const int n = la + lb;
-  // stage A then B (keys and payloads)
-#pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    const int i = j * THREADS + (int)threadIdx.x;
-    if (i < la) sk[i] = ak[i];
-    else if (i < n) sk[i] = bk[i - la];
-  }
+  // stage A then B (keys and payloads, padded layout): every load is issued
+  // into registers before the first shared-memory store, so all are in flight
   P *sv = nullptr;
-  if constexpr (has_payload<P>()) {
-    sv = reinterpret_cast<P *>(smem + align_up(sizeof(K) * T, 16));
+  {
+    K tk[ITEMS];
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
       const int i = j * THREADS + (int)threadIdx.x;
-      if (i < la) sv[i] = av[i];
-      else if (i < n) sv[i] = bv[i - la];
+      const K *src = i < la ? ak + i : bk + (i - la);
+      tk[j] = i < n ? __ldg(src) : K();
+    }
+    if constexpr (has_payload<P>()) {
+      sv = reinterpret_cast<P *>(smem + align_up(sizeof(K) * padded_len(T), 16));
+      P tv[ITEMS];
+#pragma unroll
+      for (int j = 0; j < ITEMS; ++j) {
+        const int i = j * THREADS + (int)threadIdx.x;
+        const P *src = i < la ? av + i : bv + (i - la);
+        tv[j] = i < n ? __ldg(src) : P();
+      }
+#pragma unroll
+      for (int j = 0; j < ITEMS; ++j) {
+        const int i = j * THREADS + (int)threadIdx.x;
+        if (i < n) sv[pad32(i)] = tv[j];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const int i = j * THREADS + (int)threadIdx.x;
+      if (i < n) sk[pad32(i)] = tk[j];
     }
   }
   __syncthreads();
@@ -141,26 +193,27 @@ __device__ __forceinline__ void merge_tile(const K *ak, const P *av, int la, con
   int src[ITEMS];
   const int valid = n - d;
   if (valid > 0) {
-    const int ia = merge_path<K, int>(sk, la, sk + la, lb, d);
-    serial_merge<ITEMS>(sk, la, lb, ia, d - ia, keys, src, valid);
+    const PView<K> pa{sk, 0}, pb{sk, la};  // B follows A in the unpadded numbering
+    const int ia = merge_path<K, int>(pa, la, pb, lb, d);
+    serial_merge<ITEMS, K>(pa, la, lb, ia, d - ia, keys, src, valid);
   }
   P vals[ITEMS];
   if constexpr (has_payload<P>()) {
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i)
-      if (i < valid) vals[i] = sv[src[i]];
+      if (i < valid) vals[i] = sv[pad32(src[i])];
   }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     if (i < valid) {
-      sk[d + i] = keys[i];
-      if constexpr (has_payload<P>()) sv[d + i] = vals[i];
+      sk[pad32(d + i)] = keys[i];
+      if constexpr (has_payload<P>()) sv[pad32(d + i)] = vals[i];
     }
   }
   __syncthreads();
-  stage_out<THREADS>(ok, sk, n);
-  if constexpr (has_payload<P>()) stage_out<THREADS>(ov, sv, n);
+  stage_out_padded<THREADS>(ok, sk, n);
+  if constexpr (has_payload<P>()) stage_out_padded<THREADS>(ov, sv, n);
 }
 
 }  // namespace bk

@@ -23,7 +23,8 @@ struct MergeCfg {
 
 template <typename K, typename P>
 constexpr size_t merge_smem_bytes() {
-  return align_up(sizeof(K) * MergeCfg<K>::TILE, 16) + (size_t)payload_bytes<P>() * MergeCfg<K>::TILE;
+  return align_up(sizeof(K) * padded_len(MergeCfg<K>::TILE), 16) +
+         (size_t)payload_bytes<P>() * padded_len(MergeCfg<K>::TILE);
 }
 
 // parts[k] = number of A elements among the first min(k*TILE, na+nb) outputs.

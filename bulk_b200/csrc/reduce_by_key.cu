@@ -140,8 +140,25 @@ struct Chunk {
   bool valid[E];
 };
 
-// Reads chunk `chunk` of a staged tile and derives head/tail flags.  The key
-// before the tile is hb[0][KC-1], the key after it hb[1][0].
+// dst[0 .. B) = the B-byte chunk number `chunk` of src (B = 8 or 16).
+template <int B, typename T>
+__device__ __forceinline__ void load_chunk(T *dst, const T *src, uint32_t chunk) {
+  static_assert(B == 8 || B == 16, "8- or 16-byte chunks");
+  if constexpr (B == 16) {
+    const uint4 q = reinterpret_cast<const uint4 *>(src)[chunk];
+    memcpy(dst, &q, 16);
+  } else {
+    const uint2 q = reinterpret_cast<const uint2 *>(src)[chunk];
+    memcpy(dst, &q, 8);
+  }
+}
+
+// Reads chunk `chunk` of a staged tile (one vector load of keys and one of
+// values per lane, conflict-free) and derives head/tail flags.  Neighbouring
+// keys come from the adjacent lanes by shuffles; lane 0 / lane 31 read the
+// key before / after the row from shared memory, or the halo at the tile's
+// edges (hb[0][KC-1] precedes the tile, hb[1][0] follows it).  All 32 lanes of
+// the warp call it together, for consecutive chunks.
 template <typename K, typename V>
 __device__ __forceinline__ void rbk_read_chunk(const unsigned char *buf, const K (*hb)[16 / sizeof(K)], uint64_t base,
                                                uint32_t count, uint64_t n, uint32_t chunk,
@@ -149,16 +166,26 @@ __device__ __forceinline__ void rbk_read_chunk(const unsigned char *buf, const K
   using C = RbkCfg<K, V>;
   constexpr int E = C::E;
   constexpr int KC = 16 / sizeof(K);
+  const int lane = threadIdx.x & 31;
   const K *sk = reinterpret_cast<const K *>(buf);
   const V *sv = reinterpret_cast<const V *>(buf + C::KEY_BYTES);
   const uint32_t e0 = chunk * E;
+  // one vector load each: E keys and E values (8 or 16 bytes per lane)
+  load_chunk<E * sizeof(K)>(ch.key, sk, chunk);
+  load_chunk<E * sizeof(V)>(ch.val, sv, chunk);
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     ch.valid[j] = e0 + j < count;
-    ch.key[j] = ch.valid[j] ? sk[e0 + j] : K();
-    ch.val[j] = ch.valid[j] ? sv[e0 + j] : V(0);
+    if (!ch.valid[j]) {
+      ch.key[j] = K();
+      ch.val[j] = V(0);
+    }
   }
-  const K prev = e0 == 0 ? hb[0][KC - 1] : (e0 <= count ? sk[e0 - 1] : K());
+  // neighbours across lanes
+  K prev = shfl_up(ch.key[E - 1], 1);
+  K next = shfl_down_any(ch.key[0], 1);
+  if (lane == 0) prev = e0 == 0 ? hb[0][KC - 1] : (e0 <= count ? sk[e0 - 1] : K());
+  if (lane == 31) next = e0 + E < count ? sk[e0 + E] : hb[1][0];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     const uint64_t g = base + e0 + j;
@@ -166,7 +193,7 @@ __device__ __forceinline__ void rbk_read_chunk(const unsigned char *buf, const K
     ch.head[j] = ch.valid[j] && (g == 0 || !(ch.key[j] == pk));
     // successor: inside the tile, or the first key after it
     const uint32_t nx = e0 + j + 1;
-    const K nk = nx < count ? (j + 1 < E ? ch.key[j + 1] : sk[nx]) : hb[1][0];
+    const K nk = nx < count ? (j + 1 < E ? ch.key[j + 1] : next) : hb[1][0];
     ch.tail[j] = ch.valid[j] && (g + 1 >= n || !(nk == ch.key[j]));
   }
 }

@@ -32,11 +32,13 @@ struct SortCfg {
 
 template <typename K, typename P>
 constexpr size_t bs_smem_bytes() {
-  return align_up(sizeof(K) * SortCfg<K>::BS_TILE, 16) + (size_t)payload_bytes<P>() * SortCfg<K>::BS_TILE;
+  return align_up(sizeof(K) * padded_len(SortCfg<K>::BS_TILE), 16) +
+         (size_t)payload_bytes<P>() * padded_len(SortCfg<K>::BS_TILE);
 }
 template <typename K, typename P>
 constexpr size_t mp_smem_bytes() {
-  return align_up(sizeof(K) * SortCfg<K>::MP_TILE, 16) + (size_t)payload_bytes<P>() * SortCfg<K>::MP_TILE;
+  return align_up(sizeof(K) * padded_len(SortCfg<K>::MP_TILE), 16) +
+         (size_t)payload_bytes<P>() * padded_len(SortCfg<K>::MP_TILE);
 }
 
 // Stable sort of one tile: in -> out (may alias).
@@ -46,19 +48,32 @@ __global__ void __launch_bounds__(kBsThreads) block_sort_kernel(const K *in_k, c
   constexpr int ITEMS = SortCfg<K>::BS_ITEMS, TILE = SortCfg<K>::BS_TILE;
   extern __shared__ __align__(16) unsigned char smem[];
   K *sk = reinterpret_cast<K *>(smem);
-  P *sv = reinterpret_cast<P *>(smem + align_up(sizeof(K) * TILE, 16));
+  P *sv = reinterpret_cast<P *>(smem + align_up(sizeof(K) * padded_len(TILE), 16));  // padded layout
   const uint64_t base = (uint64_t)blockIdx.x * TILE;
   const int count = (int)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
   const int tid = threadIdx.x;
 
-  // stage in; pad a partial tile with the largest key (kept after real keys)
+  // stage in (all loads in flight before the first store); pad a partial
+  // tile with the largest key (kept after real keys)
+  {
+    K tk[ITEMS];
 #pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    const int i = j * kBsThreads + tid;
-    sk[i] = i < count ? in_k[base + i] : key_max<K>();
-    if constexpr (has_payload<P>()) {
-      if (i < count) sv[i] = in_v[base + i];
+    for (int j = 0; j < ITEMS; ++j) {
+      const int i = j * kBsThreads + tid;
+      tk[j] = i < count ? __ldg(in_k + base + i) : key_max<K>();
     }
+    if constexpr (has_payload<P>()) {
+      P tv[ITEMS];
+#pragma unroll
+      for (int j = 0; j < ITEMS; ++j) {
+        const int i = j * kBsThreads + tid;
+        tv[j] = i < count ? __ldg(in_v + base + i) : P();
+      }
+#pragma unroll
+      for (int j = 0; j < ITEMS; ++j) sv[pad32(j * kBsThreads + tid)] = tv[j];
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) sk[pad32(j * kBsThreads + tid)] = tk[j];
   }
   __syncthreads();
 
@@ -67,8 +82,8 @@ __global__ void __launch_bounds__(kBsThreads) block_sort_kernel(const K *in_k, c
   P v[ITEMS];
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    k[i] = sk[tid * ITEMS + i];
-    if constexpr (has_payload<P>()) v[i] = sv[tid * ITEMS + i];
+    k[i] = sk[pad32(tid * ITEMS + i)];
+    if constexpr (has_payload<P>()) v[i] = sv[pad32(tid * ITEMS + i)];
   }
 #pragma unroll
   for (int r = 0; r < ITEMS; ++r) {
@@ -86,20 +101,20 @@ __global__ void __launch_bounds__(kBsThreads) block_sort_kernel(const K *in_k, c
     __syncthreads();  // everyone has read the previous stage
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-      sk[tid * ITEMS + i] = k[i];
-      if constexpr (has_payload<P>()) sv[tid * ITEMS + i] = v[i];
+      sk[pad32(tid * ITEMS + i)] = k[i];
+      if constexpr (has_payload<P>()) sv[pad32(tid * ITEMS + i)] = v[i];
     }
     __syncthreads();  // the stage is complete before anyone merges from it
     const int d = tid * ITEMS;
     const int p0 = d & ~(2 * w - 1);
     const int diag = d - p0;
-    const K *s = sk + p0;
-    const int ia = merge_path<K, int>(s, w, s + w, w, diag);
+    const PView<K> pa{sk, p0}, pb{sk, p0 + w};
+    const int ia = merge_path<K, int>(pa, w, pb, w, diag);
     int src[ITEMS];
-    serial_merge<ITEMS>(s, w, w, ia, diag - ia, k, src, ITEMS);
+    serial_merge<ITEMS, K>(pa, w, w, ia, diag - ia, k, src, ITEMS);
     if constexpr (has_payload<P>()) {
 #pragma unroll
-      for (int i = 0; i < ITEMS; ++i) v[i] = sv[p0 + src[i]];
+      for (int i = 0; i < ITEMS; ++i) v[i] = sv[pad32(p0 + src[i])];
     }
   }
 
@@ -107,12 +122,12 @@ __global__ void __launch_bounds__(kBsThreads) block_sort_kernel(const K *in_k, c
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    sk[tid * ITEMS + i] = k[i];
-    if constexpr (has_payload<P>()) sv[tid * ITEMS + i] = v[i];
+    sk[pad32(tid * ITEMS + i)] = k[i];
+    if constexpr (has_payload<P>()) sv[pad32(tid * ITEMS + i)] = v[i];
   }
   __syncthreads();
-  stage_out<kBsThreads>(out_k + base, sk, count);
-  if constexpr (has_payload<P>()) stage_out<kBsThreads>(out_v + base, sv, count);
+  stage_out_padded<kBsThreads>(out_k + base, sk, count);
+  if constexpr (has_payload<P>()) stage_out_padded<kBsThreads>(out_v + base, sv, count);
 }
 
 // Merge pass: runs of width w in `src` -> runs of 2w in `dst`.
