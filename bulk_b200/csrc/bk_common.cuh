@@ -276,5 +276,16 @@ inline bool aligned_to(const void *p) {
 
 inline int launch_status() { return from_cuda(cudaGetLastError()); }
 
+// Opt a kernel into `bytes` of dynamic shared memory and the largest shared
+// memory carveout (the L1 / shared split), so that as many CTAs as the
+// shared memory allows are resident.
+template <typename Kern>
+inline int set_smem_attrs(Kern kern, size_t bytes) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+  return from_cuda(e);
+}
+
 }  // namespace host
 }  // namespace bk

@@ -39,7 +39,7 @@ __global__ void merge_partition_kernel(const K *a, uint64_t na, const K *b, uint
 }
 
 template <typename K, typename P>
-__global__ void __launch_bounds__(kMergeThreads) merge_kernel(const K *a, const P *av, uint64_t na, const K *b,
+__global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(const K *a, const P *av, uint64_t na, const K *b,
                                                               const P *bv, uint64_t nb, K *out, P *outv,
                                                               const uint64_t *parts) {
   constexpr int TILE = MergeCfg<K>::TILE;
@@ -89,8 +89,7 @@ int merge_launch(const K *a, const P *av, uint64_t na, const K *b, const P *bv, 
   constexpr size_t smem = merge_smem_bytes<K, P>();
   static thread_local bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(merge_kernel<K, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return (int)e;
+    if ((st = host::set_smem_attrs(merge_kernel<K, P>, smem)) != BK_OK) return st;
     attr_set = true;
   }
   merge_kernel<K, P><<<(unsigned)tiles, kMergeThreads, smem, stream>>>(a, av, na, b, bv, nb, out, outv, parts);

@@ -44,12 +44,12 @@ struct OpSeg {
 
 constexpr int kRbkWarps = 8;
 constexpr int kRbkThreads = 32 * (kRbkWarps + 1);  // + control warp
-constexpr int kRbkRows = 4;
 
 template <typename K, typename V>
 struct RbkCfg {
-  static constexpr int E = 16 / (sizeof(K) > sizeof(V) ? sizeof(K) : sizeof(V));  // elements per lane chunk
-  static constexpr int TILE = kRbkWarps * kRbkRows * 32 * E;                     // 4096 or 2048
+  // each lane owns M consecutive elements: 64 bytes of the wider of key/value
+  static constexpr int M = 64 / (sizeof(K) > sizeof(V) ? sizeof(K) : sizeof(V));  // 16 or 8
+  static constexpr int TILE = kRbkWarps * 32 * M;                                  // 4096 or 2048
   static constexpr size_t KEY_BYTES = align_up(sizeof(K) * TILE, 128);
   static constexpr size_t BUF_BYTES = KEY_BYTES + align_up(sizeof(V) * TILE, 128);
   using P = Seg<V>;
@@ -130,72 +130,104 @@ __device__ __forceinline__ void rbk_sync_load(const K *keys, const V *vals, uint
   }
 }
 
-// The per-element scan state of one lane chunk (E consecutive elements).
-template <typename K, typename V, int E>
-struct Chunk {
-  K key[E];
-  V val[E];
-  bool head[E];
-  bool tail[E];
-  bool valid[E];
-};
-
-// dst[0 .. B) = the B-byte chunk number `chunk` of src (B = 8 or 16).
+// Loads a lane's B bytes (B = 32 or 64: C = B/16 chunks of 16 bytes) starting
+// at byte offset lane_off of `base` into dst, conflict-free: eight lanes share
+// one 128-byte bank period, so lane l fetches its chunks starting at chunk
+// r = (l / (8 / C)) mod C, which gives the eight lanes of every access phase
+// distinct banks; two select stages then rotate the chunks back into order.
 template <int B, typename T>
-__device__ __forceinline__ void load_chunk(T *dst, const T *src, uint32_t chunk) {
-  static_assert(B == 8 || B == 16, "8- or 16-byte chunks");
-  if constexpr (B == 16) {
-    const uint4 q = reinterpret_cast<const uint4 *>(src)[chunk];
-    memcpy(dst, &q, 16);
-  } else {
-    const uint2 q = reinterpret_cast<const uint2 *>(src)[chunk];
-    memcpy(dst, &q, 8);
-  }
-}
-
-// Reads chunk `chunk` of a staged tile (one vector load of keys and one of
-// values per lane, conflict-free) and derives head/tail flags.  Neighbouring
-// keys come from the adjacent lanes by shuffles; lane 0 / lane 31 read the
-// key before / after the row from shared memory, or the halo at the tile's
-// edges (hb[0][KC-1] precedes the tile, hb[1][0] follows it).  All 32 lanes of
-// the warp call it together, for consecutive chunks.
-template <typename K, typename V>
-__device__ __forceinline__ void rbk_read_chunk(const unsigned char *buf, const K (*hb)[16 / sizeof(K)], uint64_t base,
-                                               uint32_t count, uint64_t n, uint32_t chunk,
-                                               Chunk<K, V, RbkCfg<K, V>::E> &ch) {
-  using C = RbkCfg<K, V>;
-  constexpr int E = C::E;
-  constexpr int KC = 16 / sizeof(K);
-  const int lane = threadIdx.x & 31;
-  const K *sk = reinterpret_cast<const K *>(buf);
-  const V *sv = reinterpret_cast<const V *>(buf + C::KEY_BYTES);
-  const uint32_t e0 = chunk * E;
-  // one vector load each: E keys and E values (8 or 16 bytes per lane)
-  load_chunk<E * sizeof(K)>(ch.key, sk, chunk);
-  load_chunk<E * sizeof(V)>(ch.val, sv, chunk);
+__device__ __forceinline__ void load_lane_rotated(T *dst, const unsigned char *base, uint32_t lane_off, int lane) {
+  constexpr int C = B / 16;
+  static_assert(C == 2 || C == 4, "two or four 16-byte chunks");
+  const int r = (lane / (8 / C)) & (C - 1);
+  uint4 q[C];
 #pragma unroll
-  for (int j = 0; j < E; ++j) {
-    ch.valid[j] = e0 + j < count;
-    if (!ch.valid[j]) {
-      ch.key[j] = K();
-      ch.val[j] = V(0);
+  for (int k = 0; k < C; ++k) q[k] = *reinterpret_cast<const uint4 *>(base + lane_off + 16 * ((k + r) & (C - 1)));
+  // q[k] holds chunk (k + r) mod C; rotate right by r so q[c] holds chunk c
+  if (r & 1) {
+    const uint4 t = q[C - 1];
+#pragma unroll
+    for (int k = C - 1; k > 0; --k) q[k] = q[k - 1];
+    q[0] = t;
+  }
+  if constexpr (C == 4) {
+    if (r & 2) {
+      const uint4 t0 = q[0], t1 = q[1];
+      q[0] = q[2];
+      q[1] = q[3];
+      q[2] = t0;
+      q[3] = t1;
     }
   }
-  // neighbours across lanes
-  K prev = shfl_up(ch.key[E - 1], 1);
-  K next = shfl_down_any(ch.key[0], 1);
-  if (lane == 0) prev = e0 == 0 ? hb[0][KC - 1] : (e0 <= count ? sk[e0 - 1] : K());
-  if (lane == 31) next = e0 + E < count ? sk[e0 + E] : hb[1][0];
+  memcpy(dst, q, B);
+}
+
+// A lane's M consecutive elements of a staged tile, with head / tail flags.
+template <typename K, typename V, int M>
+struct LaneRun {
+  K key[M];
+  V val[M];
+  uint32_t head;  // bit j: element j starts a run
+  uint32_t tail;  // bit j: element j ends a run
+  int nvalid;     // elements of this lane inside the tile
+};
+
+// Element index of the lane's first element: e0 = (warp * 32 + lane) * M.
+// Neighbouring keys come from the adjacent lanes by shuffles; lane 0 / lane
+// 31 read the key before / after the warp's range from shared memory, or the
+// halo at the tile's edges (hb[0][KC-1] precedes the tile, hb[1][0] follows
+// it).  first_tile: the tile starts the input; last_tile: it ends it.
+template <typename K, typename V>
+__device__ __forceinline__ void rbk_read_lane(const unsigned char *buf, const K (*hb)[16 / sizeof(K)], uint32_t count,
+                                              bool first_tile, bool last_tile, int warp, int lane,
+                                              LaneRun<K, V, RbkCfg<K, V>::M> &lr) {
+  using C = RbkCfg<K, V>;
+  constexpr int M = C::M;
+  constexpr int KC = 16 / sizeof(K);
+  const K *sk = reinterpret_cast<const K *>(buf);
+  const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
+  load_lane_rotated<M * sizeof(K)>(lr.key, buf, e0 * (uint32_t)sizeof(K), lane);
+  load_lane_rotated<M * sizeof(V)>(lr.val, buf + C::KEY_BYTES, e0 * (uint32_t)sizeof(V), lane);
+  const int nvalid = (int)min(max((int)count - (int)e0, 0), M);
+  lr.nvalid = nvalid;
 #pragma unroll
-  for (int j = 0; j < E; ++j) {
-    const uint64_t g = base + e0 + j;
-    const K pk = j == 0 ? prev : ch.key[j - 1];
-    ch.head[j] = ch.valid[j] && (g == 0 || !(ch.key[j] == pk));
-    // successor: inside the tile, or the first key after it
-    const uint32_t nx = e0 + j + 1;
-    const K nk = nx < count ? (j + 1 < E ? ch.key[j + 1] : next) : hb[1][0];
-    ch.tail[j] = ch.valid[j] && (g + 1 >= n || !(nk == ch.key[j]));
+  for (int j = 0; j < M; ++j)
+    if (j >= nvalid) {
+      lr.key[j] = K();
+      lr.val[j] = V(0);
+    }
+  K prev = shfl_up(lr.key[M - 1], 1);
+  K next = shfl_down_any(lr.key[0], 1);
+  if (lane == 0) prev = e0 == 0 ? hb[0][KC - 1] : sk[e0 - 1];
+  if (lane == 31) next = e0 + M < count ? sk[e0 + M] : hb[1][0];
+  uint32_t head = 0, tail = 0;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const K pk = j == 0 ? prev : lr.key[j - 1];
+    const bool h = (j < nvalid) && !(lr.key[j] == pk);
+    head |= (uint32_t)h << j;
+    // successor inside the lane, in the next lane / warp, or after the tile
+    const bool last_of_tile = (e0 + j + 1 == count);
+    const K nk = j + 1 < M ? lr.key[j + 1] : next;
+    const bool t = (j < nvalid) && (last_of_tile ? (last_tile || !(hb[1][0] == lr.key[j])) : !(nk == lr.key[j]));
+    tail |= (uint32_t)t << j;
   }
+  if (first_tile && e0 == 0 && nvalid > 0) head |= 1u;  // the input's first element
+  lr.head = head;
+  lr.tail = tail;
+}
+
+// (c, v) of a lane's elements folded in order.
+template <typename K, typename V, int M>
+__device__ __forceinline__ Seg<V> lane_fold(const LaneRun<K, V, M> &lr) {
+  uint32_t c = __popc(lr.head);
+  V v = V(0);
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    if (lr.head & (1u << j)) v = lr.val[j];
+    else v = (V)(v + lr.val[j]);
+  }
+  return Seg<V>{c, v};
 }
 
 template <typename K, typename V>
@@ -207,7 +239,7 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
                                                              unsigned int num_tiles) {
   using C = RbkCfg<K, V>;
   using P = typename C::P;
-  constexpr int E = C::E, TILE = C::TILE, R = kRbkRows;
+  constexpr int M = C::M, TILE = C::TILE;
   constexpr unsigned int NONE = 0xffffffffu;
   OpSeg<V> op;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -290,21 +322,10 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
       if (!control) {
         const uint64_t base = (uint64_t)t * TILE;
         const uint32_t count = (uint32_t)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
-        P wagg = OpSeg<V>::identity();
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
-          Chunk<K, V, E> ch;
-          rbk_read_chunk<K, V>(buf[slot], s_halo[slot], base, count, n, chunk, ch);
-          P a = OpSeg<V>::identity();
-#pragma unroll
-          for (int j = 0; j < E; ++j) {
-            if (ch.valid[j]) a = op(a, P{ch.head[j] ? 1u : 0u, ch.val[j]});
-          }
-          const P incl = warp_inclusive_scan(a, op, lane);
-          wagg = op(wagg, shfl_idx_any(incl, 31));
-        }
-        if (lane == 0) s_wagg[slot][warp] = wagg;
+        LaneRun<K, V, M> lr;
+        rbk_read_lane<K, V>(buf[slot], s_halo[slot], count, t == 0, base + count == n, warp, lane, lr);
+        const P incl = warp_inclusive_scan(lane_fold(lr), op, lane);
+        if (lane == 31) s_wagg[slot][warp] = incl;
       }
     }
     __syncthreads();
@@ -314,6 +335,8 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
       for (int i = 0; i < kRbkWarps; ++i) agg_t = op(agg_t, s_wagg[slot][i]);
     }
 
+    LaneRun<K, V, M> lr2;                // phase-2 lane data, kept across the barrier
+    P lane_incl = OpSeg<V>::identity();  // its inclusive scan over the warp's lanes
     if (control) {
       if (leader && t != NONE && !s_abort && (long long)t != skip_publish_tile)
         st.publish(t, t == 0 ? kStPrefix : kStAggregate, agg_t);
@@ -336,6 +359,7 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
         }
       }
     } else if (pending != NONE) {
+      // phase 2, the part that needs no prefix: overlaps the look-back
       if (inflight & 4u) {
         if (!mbar_wait(&s_bar[2], parity[2], spin_limit_ns)) {
           record_error(hdr, BK_ERR_SPIN_TIMEOUT, pending);
@@ -344,8 +368,12 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
         parity[2] ^= 1u;
         inflight &= ~4u;
       }
+      const uint64_t base = (uint64_t)pending * TILE;
+      const uint32_t count = (uint32_t)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
+      rbk_read_lane<K, V>(buf[2], s_halo[2], count, pending == 0, base + count == n, warp, lane, lr2);
+      lane_incl = warp_inclusive_scan(lane_fold(lr2), op, lane);
     }
-    __syncthreads();  // the prefix is known; the phase-2 tile is staged
+    __syncthreads();  // the prefix is known
     if (s_abort) break;
 
     // ---- phase 2 of the pending tile: emit its runs
@@ -354,33 +382,29 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
       const uint32_t count = (uint32_t)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
       P carry = s_prefix;
       for (int i = 0; i < warp; ++i) carry = op(carry, s_wagg[slot ^ 1][i]);
+      const bool last_tile = base + count == n;
+      const LaneRun<K, V, M> &lr = lr2;
+      const P excl = shfl_up(lane_incl, 1);
+      if (lane > 0) carry = op(carry, excl);
+      // walk the lane's elements with the running (c, v); each tail emits its run
+      const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
+      uint32_t c = carry.c;
+      V v = carry.v;
 #pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
-        Chunk<K, V, E> ch;
-        rbk_read_chunk<K, V>(buf[2], s_halo[2], base, count, n, chunk, ch);
-        P loc[E];
-        P a = OpSeg<V>::identity();
-#pragma unroll
-        for (int j = 0; j < E; ++j) {
-          if (ch.valid[j]) a = op(a, P{ch.head[j] ? 1u : 0u, ch.val[j]});
-          loc[j] = a;
-        }
-        const P incl = warp_inclusive_scan(a, op, lane);
-        P excl = shfl_up(incl, 1);
-        if (lane == 0) excl = OpSeg<V>::identity();
-        const P pre = op(carry, excl);
-#pragma unroll
-        for (int j = 0; j < E; ++j) {
-          if (ch.tail[j]) {
-            const P r = op(pre, loc[j]);
-            const uint64_t slot_out = (uint64_t)r.c - 1;
-            out_keys[slot_out] = ch.key[j];
-            out_vals[slot_out] = r.v;
-            if (base + chunk * E + j == n - 1) *d_num_out = r.c;
+      for (int j = 0; j < M; ++j) {
+        if (j < lr.nvalid) {
+          if (lr.head & (1u << j)) {
+            ++c;
+            v = lr.val[j];
+          } else {
+            v = (V)(v + lr.val[j]);
+          }
+          if (lr.tail & (1u << j)) {
+            out_keys[c - 1] = lr.key[j];
+            out_vals[c - 1] = v;
+            if (last_tile && e0 + j + 1 == count) *d_num_out = c;
           }
         }
-        carry = op(carry, shfl_idx_any(incl, 31));
       }
     }
 
@@ -427,8 +451,7 @@ int rbk_launch(const K *keys, const V *vals, uint64_t n, K *out_keys, V *out_val
   const size_t smem = 3 * C::BUF_BYTES;
   static thread_local bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(rbk_kernel<K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return (int)e;
+    if ((st = host::set_smem_attrs(rbk_kernel<K, V>, smem)) != BK_OK) return st;
     attr_set = true;
   }
   const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * 2);

@@ -377,8 +377,7 @@ int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t 
   const size_t smem = 3 * (size_t)C::TILE_BYTES;
   static thread_local bool attr_set = false;  // per host thread; cheap and idempotent
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(scan_kernel<T, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return (int)e;
+    if ((st = host::set_smem_attrs(scan_kernel<T, Op>, smem)) != BK_OK) return st;
     attr_set = true;
   }
   const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * 2);

@@ -145,7 +145,7 @@ __global__ void sort_partition_kernel(const K *keys, uint64_t n, uint64_t w, uin
 }
 
 template <typename K, typename P>
-__global__ void __launch_bounds__(kMpThreads) sort_merge_kernel(const K *sk, const P *sv, K *dk, P *dv, uint64_t n,
+__global__ void __launch_bounds__(kMpThreads, 4) sort_merge_kernel(const K *sk, const P *sv, K *dk, P *dv, uint64_t n,
                                                                 uint64_t w, const uint64_t *parts,
                                                                 uint64_t num_tiles) {
   constexpr uint64_t T = SortCfg<K>::MP_TILE;
@@ -177,7 +177,7 @@ size_t sort_ws_bytes_t(uint64_t n) {
 
 template <typename Kern>
 static int set_smem(Kern kern, size_t bytes) {
-  return host::from_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return host::set_smem_attrs(kern, bytes);
 }
 
 template <typename K, typename P>
