@@ -119,49 +119,70 @@ def run_reference(args):
 
 
 def cpu_reference_time(n_sample: int, steps: int, warmup: int, threads: int):
-    """Seconds per sample-step of reduce + scan over n_sample elements of each dtype."""
+    """Seconds per sample-step of reduce + scan over n_sample elements of each
+    dtype, and which implementation ran ("reference": the reference's own
+    algorithms compiled for the host, oracle/_ref; else "port": the oracle's
+    threaded restatement)."""
     import ctypes
 
     import numpy as np
 
-    from oracle import _lib as olib  # CPU baseline leg: the oracle's threaded restatement
-    import oracle
-    red = olib.bko_baseline_reduce
-    red.restype = ctypes.c_double
-    red.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
-    scn = olib.bko_baseline_inclusive_scan
-    scn.restype = None
-    scn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
-    data = [(oracle.gen(np.float32, n_sample, 0, -1.0, 1.0), 0), (oracle.gen(np.float64, n_sample, 0, -1.0, 1.0), 1),
-            (oracle.gen(np.int32, n_sample, 0, -100, 100), 2)]
-    outs = [np.empty_like(x) for x, _ in data]
+    import oracle  # CPU baseline leg only
+    from oracle import reference as R
+    data = [oracle.gen(np.float32, n_sample, 0, -1.0, 1.0), oracle.gen(np.float64, n_sample, 0, -1.0, 1.0),
+            oracle.gen(np.int32, n_sample, 0, -100, 100)]
+    outs = [np.empty_like(x) for x in data]
+    if R.available():
+        kind = "reference"
 
-    def step():
-        for (x, t), o in zip(data, outs):
-            red(x.ctypes.data, x.size, t, threads)
-            scn(x.ctypes.data, o.ctypes.data, x.size, t, threads)
+        def step():
+            for x, o in zip(data, outs):
+                R.cpu_reduce(x, x.dtype.type(0), threads)
+                R.cpu_inclusive_scan(x, x.dtype.type(0), threads, out=o)
+    else:
+        kind = "port"
+        olib = oracle._lib
+        red = olib.bko_baseline_reduce
+        red.restype = ctypes.c_double
+        red.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+        scn = olib.bko_baseline_inclusive_scan
+        scn.restype = None
+        scn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+
+        def step():
+            for t, (x, o) in enumerate(zip(data, outs)):
+                red(x.ctypes.data, x.size, t, threads)
+                scn(x.ctypes.data, o.ctypes.data, x.size, t, threads)
 
     for _ in range(warmup):
         step()
+    if steps <= 0:  # size the sample to about 10 s of CPU work
+        t0 = time.perf_counter()
+        step()
+        steps = int(min(50, max(1, 10.0 / max(time.perf_counter() - t0, 1e-3))))
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
-    return (time.perf_counter() - t0) / steps
+    return (time.perf_counter() - t0) / steps, kind, steps
 
 
 def cpu_reference_line(steps, warmup):
+    """steps <= 0: as many sample steps as fill about 10 s."""
     threads = os.cpu_count() or 1
     n_sample = 1 << 24
-    sec = cpu_reference_time(n_sample, max(1, steps), max(1, min(warmup, 3)), threads)
+    sec, kind, steps = cpu_reference_time(n_sample, steps, max(1, min(warmup, 3)), threads)
     bytes_per = sum(3 * n_sample * s for _, s in DTYPES)
     gbs = bytes_per / sec / 1e9
+    what = ("the reference's agent-level reduce / inclusive_scan compiled for the host, over the drivers' "
+            "partitioning (reduce.cu, scan.cu)" if kind == "reference" else "the oracle's threaded restatement")
     sample = (f"reduce+inclusive_scan over 2^24 elements of each of f32/f64/i32 (1/16 of the 2^28 workload), "
-              f"{threads} threads, partitioned like reduce.cu/scan.cu")
+              f"{threads} threads, {what}")
     return {"metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": 0, "steps": steps, "warmup": warmup,
             "ms_per_step": sec * 1e3 * (N_HEADLINE / n_sample), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64+i32", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "n": N_HEADLINE, "l2": "inputs larger than L2"},
-            "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind,
+                             "sample": sample + f", {steps} timed sample steps"},
             "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -485,7 +506,7 @@ def main(argv=None):
         dist.destroy_process_group()
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
-            ref = cpu_reference_line(3, 1)
+            ref = cpu_reference_line(0, 1)
             line["cpu_baseline"] = ref["cpu_baseline"]
         print(json.dumps(line), flush=True)
     return 0
