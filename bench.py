@@ -169,13 +169,13 @@ def cpu_reference_time(n_sample: int, steps: int, warmup: int, threads: int):
 def cpu_reference_line(steps, warmup):
     """steps <= 0: as many sample steps as fill about 10 s."""
     threads = os.cpu_count() or 1
-    n_sample = 1 << 24
+    n_sample = 1 << 26
     sec, kind, steps = cpu_reference_time(n_sample, steps, max(1, min(warmup, 3)), threads)
     bytes_per = sum(3 * n_sample * s for _, s in DTYPES)
     gbs = bytes_per / sec / 1e9
     what = ("the reference's agent-level reduce / inclusive_scan compiled for the host, over the drivers' "
             "partitioning (reduce.cu, scan.cu)" if kind == "reference" else "the oracle's threaded restatement")
-    sample = (f"reduce+inclusive_scan over 2^24 elements of each of f32/f64/i32 (1/16 of the 2^28 workload), "
+    sample = (f"reduce+inclusive_scan over 2^26 elements of each of f32/f64/i32 (1/4 of the 2^28 workload), "
               f"{threads} threads, {what}")
     return {"metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": 0, "steps": steps, "warmup": warmup,
             "ms_per_step": sec * 1e3 * (N_HEADLINE / n_sample), "higher_is_better": True, "scaling": "weak",
