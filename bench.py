@@ -42,6 +42,21 @@ N_HEADLINE = 1 << 28
 DTYPES = [("f32", 4), ("f64", 8), ("i32", 4)]
 
 
+def _traffic_per_unit(kernel_case):
+    """DRAM bytes per element of a kernel, from the committed ncu summary
+    (profiles/ncu_traffic.json: dram__bytes_read.sum + dram__bytes_write.sum of
+    one captured launch on a smaller case, divided by its elements; traffic
+    grows in proportion to the elements for these streaming kernels)."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None, None
+    d = json.loads(p.read_text())
+    e = d.get(kernel_case)
+    if not e:
+        return None, None
+    return e["dram_bytes_per_unit"], e["case"]
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -484,6 +499,9 @@ def main(argv=None):
     line = None
     if rank == 0:
         achieved = algo_bytes[dom] / (per[dom] * 1e-3) / 1e9
+        tcase = {("f32", "scan"): "scan_kernel_0", ("f64", "scan"): "scan_kernel_1", ("i32", "reduce"): "reduce_kernel_2"}
+        bpu, tsrc = _traffic_per_unit(tcase.get(dom, ""))
+        traffic = bpu * n if bpu is not None else None
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -494,7 +512,9 @@ def main(argv=None):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "kernel": f"{dom[1]}_{dom[0]}", "algorithmic_bytes_per_launch": algo_bytes[dom],
-                         "traffic": None},
+                         "traffic": traffic,
+                         "traffic_source": (f"profiles/ncu_traffic.json ({tsrc}), scaled to {n} elements"
+                                            if traffic is not None else None)},
             "ops": ops,
             "e2e": {"value": bytes_step / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps},
