@@ -75,6 +75,16 @@ __device__ __forceinline__ uint4 ld_stream_v4(const void *p) {
       : "l"(p));
   return r;
 }
+// 16-byte load through L1 without allocating there, with an L2 eviction
+// policy (createpolicy); coherent, so the source may be written later in the
+// same kernel.
+__device__ __forceinline__ uint4 ld_v4_l2hint(const void *p, uint64_t policy) {
+  uint4 r;
+  asm("ld.global.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(p), "l"(policy));
+  return r;
+}
 // Streaming 16-byte store (evict-first).
 __device__ __forceinline__ void st_stream_v4(void *p, uint4 v) {
   asm volatile("st.global.cs.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(v.x), "r"(v.y), "r"(v.z),
@@ -102,6 +112,20 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
 }
 __device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Acquire / release on a CTA-local word (shared memory, generic address).
+__device__ __forceinline__ unsigned int ld_acquire_cta_u32(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.acquire.cta.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_cta_u32(unsigned int *p, unsigned int v) {
+  asm volatile("st.release.cta.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Barrier `id` (1-15; 0 is __syncthreads) over the first `threads` threads
+// that reach it; every participating warp must take part with all its lanes.
+__device__ __forceinline__ void named_barrier_sync(int id, int threads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 __device__ __forceinline__ int ld_relaxed_s32(const int *p) {
   int v;

@@ -7,12 +7,13 @@
 // moves the minimum 2*N*s (read once, write once).
 //
 // Per tile (32 KB): an atomic ticket names the tile (launch order, so every
-// predecessor is already running); one TMA bulk copy brings the tile into
-// shared memory; each warp scans its rows of 16-byte chunks with shuffles;
-// the tile publishes its aggregate, warp 0 looks back over its predecessors
-// for the exclusive prefix (bk_lookback.cuh) and publishes the inclusive
-// prefix; the results leave with one TMA bulk store.  A tiny init kernel
-// clears the tile status words before each scan.
+// predecessor is already running); a TMA bulk copy brings it into shared
+// memory, where the compute warps reduce it and the tile publishes its
+// aggregate; a dedicated look-back warp later finds its exclusive prefix
+// over the predecessors' published statuses (bk_lookback.cuh) and publishes
+// its inclusive prefix; the tile is then re-read from L2, scanned, and
+// written with one TMA bulk store.  A tiny init kernel clears the tile
+// status words before each scan.
 //
 // Semantics follow scan.cu:166-169 and bulk/algorithm/scan.hpp:455-486:
 // out[i] = init (+) in[0] (+) ... (+) in[i].
@@ -22,9 +23,12 @@
 
 namespace bk {
 
-constexpr int kScanWarps = 8;                       // compute warps
-constexpr int kScanThreads = 32 * (kScanWarps + 1);  // + one control warp
+constexpr int kScanWarps = 8;                                // compute warps (0-7)
+constexpr int kScanMainThreads = 32 * (kScanWarps + 1);      // + the loader warp (8): barrier 1
+constexpr int kScanThreads = kScanMainThreads + 32;          // + the look-back warp (9)
 constexpr int kScanRowsPerWarp = 8;
+constexpr int kScanBufs = 3;  // tile buffers in rotation (see scan_kernel)
+constexpr int kScanQueue = 4;  // look-back queue entries (more than the 2-iteration lag)
 
 template <typename T>
 struct ScanCfg {
@@ -94,23 +98,35 @@ __device__ __forceinline__ uint32_t scan_tile_count(uint64_t n, unsigned int til
   return (uint32_t)((n - base) < (uint64_t)ScanCfg<T>::TILE ? (n - base) : (uint64_t)ScanCfg<T>::TILE);
 }
 
-// Persistent two-phase scan with a control warp.  Each CTA loops over tiles
-// taken from an atomic ticket (the next ticket is always fetched one iteration
-// ahead, so its latency is hidden).  Iteration i of a CTA:
-//   * control warp: starts the TMA load of the next phase-1 tile (kept in L2
-//     with an evict-last hint) and the re-read of the previous tile p from L2
-//     (evict-first);
-//   * compute warps: phase 1 of the current tile t -- reduce it (pass A);
-//   * control warp: publishes t's aggregate (tile 0: its inclusive prefix),
-//     then looks back for p's exclusive prefix -- every predecessor's
-//     aggregate is an iteration old by now, so nothing waits on a slow load --
-//     and publishes p's inclusive prefix;
-//   * compute warps, meanwhile: scan p's rows in registers (pass B); once the
-//     prefix is known they add it and write the tile back to shared memory;
-//   * control warp: one TMA bulk store writes the tile out (evict-first).
-// A tile waiting for its prefix holds no shared memory: its data waits in L2.
-// Every wait points at a lower tile whose ticket a running CTA already took,
-// so the waits always end; each is still bounded by spin_limit_ns.
+// Persistent two-phase scan.  Warps 0-7 compute, warp 8 (lane 0) loads and
+// stores, warp 9 looks back.  Each CTA loops over tiles taken from an atomic
+// ticket (fetched one iteration ahead; the atomic's result is read only an
+// iteration later, so its latency is hidden).  Tile t_i, ticketed for
+// iteration i, lives in buffer i mod 3 and goes through:
+//   iteration i-1  loader: TMA prefetch from HBM (L2 evict-last);
+//   iteration i    compute: phase 1, the tile's reduction from shared
+//                  memory; then compute thread 0 publishes its aggregate and
+//                  queues it for the look-back warp; the loader re-reads
+//                  t_{i-1}, whose phase 1 ended an iteration ago, from L2 into
+//                  this buffer (its phase-1 data is no longer needed);
+//   iteration i+1  compute: phase 2 of t_{i-1} from this buffer -- scan,
+//                  add the prefix, write back; loader: TMA bulk store
+//                  (evict-first), after which the buffer takes the prefetch
+//                  of t_{i+2}.
+// So every TMA load is issued about an iteration before it is needed, and a
+// tile's data waits in L2, not shared memory, between its two phases.  The
+// look-back warp runs beside all this on its own: it takes queued tiles in
+// order, each one once the next has been queued (its predecessors have then
+// had an iteration to publish), and hands back the exclusive prefix through
+// a shared-memory queue two iterations after the tile's phase 1.  The compute
+// and loader warps meet at two named barriers per iteration; the look-back
+// warp meets nobody, so its L2 round trips are off their critical path.
+// Whether a tile has a TMA copy depends only on (tile, n, alignment), so
+// every thread tracks the mbarrier phases itself.  Every look-back wait
+// points at a lower tile whose ticket a running CTA already took and whose
+// aggregate depends only on its load, so the waits always end; every wait
+// (look-back, mbarrier, queue) is still bounded by spin_limit_ns, and a
+// failure anywhere stops the CTA at its next barrier.
 template <typename T, typename Op>
 __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *out, uint64_t n, T init,
                                                                typename ScanCfg<T>::Status st, WsHeader *hdr,
@@ -118,235 +134,307 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
                                                                long long skip_publish_tile, int tma_ok,
                                                                unsigned int num_tiles) {
   using C = ScanCfg<T>;
-  constexpr int V = C::V, TILE = C::TILE, R = kScanRowsPerWarp;
+  constexpr int V = C::V, TILE = C::TILE, R = kScanRowsPerWarp, NB = kScanBufs, Q = kScanQueue;
   constexpr unsigned int NONE = 0xffffffffu;
   Op op;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  T *const bufA0 = reinterpret_cast<T *>(smem_raw);
-  T *const bufA1 = bufA0 + TILE;
-  T *const bufB = bufA1 + TILE;
-  __shared__ __align__(8) uint64_t s_bar[3];  // 0, 1: phase-1 slots; 2: phase-2 buffer
-  __shared__ unsigned int s_ticket[2];
-  __shared__ int s_has_tma[3];
-  __shared__ T s_wtot[2][kScanWarps];
-  __shared__ T s_prefix;
+  T *const buf0 = reinterpret_cast<T *>(smem_raw);  // NB tile buffers
+  __shared__ __align__(8) uint64_t s_bar[NB];
+  __shared__ unsigned int s_ticket[2];   // t_i, by iteration parity
+  __shared__ T s_wtot[4][kScanWarps];    // per-warp totals of t_i, by iteration mod 4
+  __shared__ unsigned int s_q_tile[Q];   // look-back queue: entry j = t_j
+  __shared__ T s_q_agg[Q];
+  __shared__ T s_q_prefix[Q];
+  __shared__ unsigned int s_q_in, s_q_out;  // entries queued / prefixes returned
   __shared__ int s_abort;
+  __shared__ int s_abort_seen[4];        // s_abort as tid 0 saw it before each barrier 1 (two per iteration)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const bool control = (warp == kScanWarps);
-  const bool leader = control && lane == 0;
+  const bool compute = warp < kScanWarps;
+  const bool loader_warp = warp == kScanWarps;
+  const bool leader = loader_warp && lane == 0;
+  const bool lbwarp = warp == kScanWarps + 1;
+  // a TMA copy exists for `tile` exactly when this holds (scan_issue_tile_load)
+  auto has_tma = [&](unsigned int tile) -> bool {
+    return tma_ok && tile != NONE && (scan_tile_count<T>(n, tile) & ~(uint32_t)(V - 1)) != 0u;
+  };
+  auto abort_now = [&]() { *reinterpret_cast<volatile int *>(&s_abort) = 1; };
+  auto aborted = [&]() -> bool { return *reinterpret_cast<volatile int *>(&s_abort) != 0; };
 
-  unsigned int next_ticket = NONE;  // leader only: ticket for the next phase-1 load
-  bool issued_store = false;        // leader only
+  unsigned int next_raw = NONE;  // loader: next ticket, not yet range-checked
+  bool issued_store = false;     // loader
+  uint32_t issued[NB];           // loader: TMA loads issued on each of s_bar[]
+#pragma unroll
+  for (int b = 0; b < NB; ++b) issued[b] = 0u;
   uint64_t keep = 0, stream = 0;
   if (leader) {
     keep = l2_policy_evict_last();
     stream = l2_policy_evict_first();
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
-    mbar_init(&s_bar[2], 1);
+    for (int b = 0; b < NB; ++b) mbar_init(&s_bar[b], 1);
     fence_proxy_async_smem();
     s_abort = 0;
-    s_has_tma[0] = s_has_tma[1] = s_has_tma[2] = 0;
+    s_q_in = 0u;
+    s_q_out = 0u;
     const unsigned int t0 = atomicAdd(&hdr->tile_ticket, 1u);
     s_ticket[0] = t0 < num_tiles ? t0 : NONE;
     if (t0 < num_tiles) {
-      if (tma_ok) s_has_tma[0] = scan_issue_tile_load(in, n, t0, bufA0, &s_bar[0], keep);
-      const unsigned int t1 = atomicAdd(&hdr->tile_ticket, 1u);
-      next_ticket = t1 < num_tiles ? t1 : NONE;
+      if (tma_ok) issued[0] += scan_issue_tile_load(in, n, t0, buf0, &s_bar[0], keep) ? 1u : 0u;
+      next_raw = atomicAdd(&hdr->tile_ticket, 1u);
     }
   }
   __syncthreads();
 
-  uint32_t parity[3] = {0u, 0u, 0u};
-  uint32_t inflight = s_has_tma[0] ? 1u : 0u;  // bit b: a TMA load on s_bar[b] not yet waited for
-  unsigned int pending = NONE;                 // tile whose phase 2 is due this iteration
-  T pending_agg = Op::identity();
-
-  for (int it = 0;; ++it) {
-    const int slot = it & 1;
-    const unsigned int t = s_ticket[slot];
-    T *const bA = slot ? bufA1 : bufA0;
-    T *const bA_next = slot ? bufA0 : bufA1;
-
-    // ---- control: start the loads (phase-2 re-read first), fetch a ticket
-    if (leader) {
-      s_has_tma[2] = 0;
-      if (pending != NONE && tma_ok) {
-        if (issued_store) tma_store_wait_read();  // bufB free again
-        s_has_tma[2] = scan_issue_tile_load(in, n, pending, bufB, &s_bar[2], stream);
-      }
-      const unsigned int tn = (t != NONE) ? next_ticket : NONE;
-      s_ticket[slot ^ 1] = tn;
-      s_has_tma[slot ^ 1] = 0;
-      if (tn != NONE && tma_ok) s_has_tma[slot ^ 1] = scan_issue_tile_load(in, n, tn, bA_next, &s_bar[slot ^ 1], keep);
-      next_ticket = NONE;
-      if (tn != NONE) {
-        const unsigned int x = atomicAdd(&hdr->tile_ticket, 1u);  // used next iteration
-        next_ticket = x < num_tiles ? x : NONE;
-      }
-    }
-    if (!tma_ok && !control) {
-      if (t != NONE) scan_sync_tile_load(in, n, t, bA);
-      if (pending != NONE) scan_sync_tile_load(in, n, pending, bufB);
-    }
-    __syncthreads();
-    if (s_has_tma[slot ^ 1]) inflight |= 1u << (slot ^ 1);
-    if (s_has_tma[2]) inflight |= 4u;
-
-    // ---- compute: phase 1 of t (pass A)
-    if (t != NONE) {
-      if (inflight & (1u << slot)) {
-        if (!control && !mbar_wait(&s_bar[slot], parity[slot], spin_limit_ns)) {
-          record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
-          s_abort = 1;
+  if (lbwarp) {
+    // ---- the look-back warp.  Waits (bounded) until `count` entries are
+    // queued; false on an abort or a timeout.
+    auto wait_queued = [&](unsigned int count) -> bool {
+      unsigned long long w0 = 0;
+      bool ready = false;
+      for (unsigned int spins = 0;; ++spins) {
+        if (ld_acquire_cta_u32(&s_q_in) >= count) {
+          ready = true;
+          break;
         }
-        parity[slot] ^= 1u;
-        inflight &= ~(1u << slot);
-      }
-      if (!control) {
-        const uint32_t count = scan_tile_count<T>(n, t);
-        T a = Op::identity();
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
-          T x[V];
-          uint4 c = reinterpret_cast<const uint4 *>(bA)[chunk];
-          memcpy(&x[0], &c, 16);
-#pragma unroll
-          for (int j = 0; j < V; ++j)
-            if (chunk * V + j < count) a = op(a, x[j]);
-        }
-        a = warp_reduce(a, op);
-        if (lane == 0) s_wtot[slot][warp] = a;
-      }
-    }
-    __syncthreads();
-    T agg_t = Op::identity();
-    if (t != NONE) {
-      agg_t = s_wtot[slot][0];
-#pragma unroll
-      for (int i = 1; i < kScanWarps; ++i) agg_t = op(agg_t, s_wtot[slot][i]);
-    }
-
-    T y[R][V];
-    if (control) {
-      // ---- publish t's aggregate, look back for p
-      if (leader && t != NONE && !s_abort && (long long)t != skip_publish_tile) {
-        if (t == 0) st.publish(0u, kStPrefix, op(init, agg_t));
-        else st.publish(t, kStAggregate, agg_t);
-      }
-      if (pending != NONE) {
-        const unsigned int p = pending;
-        T excl = init;
-        bool ok = true;
-        if (p != 0) ok = lookback_exclusive<T>(st, p, op, excl, hdr, spin_limit_ns);
-        if (leader) {
-          if (ok) {
-            if (p != 0 && (long long)p != skip_publish_tile) st.publish(p, kStPrefix, op(excl, pending_agg));
-            s_prefix = excl;
-          } else {
-            s_abort = 1;
+        if (aborted()) break;
+        if ((spins & 15u) == 15u) {
+          const unsigned long long now = globaltimer_ns();
+          if (w0 == 0) w0 = now;
+          else if (now - w0 > spin_limit_ns) {
+            if (lane == 0) {
+              record_error(hdr, BK_ERR_SPIN_TIMEOUT, NONE);
+              abort_now();
+            }
+            break;
           }
         }
+        __nanosleep(64);
       }
-      if (pending != NONE && (inflight & 4u)) {
-        parity[2] ^= 1u;
-        inflight &= ~4u;
-      }
-    } else if (pending != NONE) {
-      // ---- pass B: p's rows in registers, offset by the earlier warps' totals
-      const uint32_t count = scan_tile_count<T>(n, pending);
-      if (inflight & 4u) {
-        if (!mbar_wait(&s_bar[2], parity[2], spin_limit_ns)) {
-          record_error(hdr, BK_ERR_SPIN_TIMEOUT, pending);
-          s_abort = 1;
+      return __all_sync(0xffffffffu, ready);
+    };
+    for (unsigned int j = 0;; ++j) {
+      if (!wait_queued(j + 1u)) break;
+      const unsigned int q = s_q_tile[j % Q];
+      if (q == NONE) break;  // tickets only grow: nothing after this
+      // a real tile is always followed by another entry; taking the tile
+      // once that entry is queued gives its predecessors an iteration to
+      // publish their aggregates
+      if (!wait_queued(j + 2u)) break;
+      const T agg = s_q_agg[j % Q];
+      T excl = init;
+      bool ok = true;
+      if (q != 0) ok = lookback_exclusive<T>(st, q, op, excl, hdr, spin_limit_ns);
+      if (lane == 0) {
+        if (ok) {
+          if (q != 0 && (long long)q != skip_publish_tile) st.publish(q, kStPrefix, op(excl, agg));
+          s_q_prefix[j % Q] = excl;
+          st_release_cta_u32(&s_q_out, j + 1u);
+        } else {
+          abort_now();
         }
-        parity[2] ^= 1u;
-        inflight &= ~4u;
       }
-      T carry = Op::identity();
-      bool have = false;
-      for (int i = 0; i < warp; ++i) {
-        carry = have ? op(carry, s_wtot[slot ^ 1][i]) : s_wtot[slot ^ 1][i];
-        have = true;
+      if (!ok) break;
+    }
+    return;
+  }
+
+  // ---- compute warps and the loader
+  uint32_t parity[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) parity[b] = 0u;
+  unsigned int p_tile = NONE, q_tile = NONE;  // t_{i-2}, t_{i-1}
+
+  for (int it = 0;; ++it) {
+    const int bt = it % NB;              // buffer of t_i
+    const int bp = (it + NB - 1) % NB;   // buffer of p = t_{i-2}: re-read there last iteration
+    const int bn = (it + 1) % NB;        // buffer for the prefetch of t_{i+1}
+    const unsigned int t = s_ticket[it & 1];
+    const unsigned int p = p_tile;
+
+    // ---- loader: prefetch t_{i+1} into the buffer whose store went out last
+    if (leader) {
+      const unsigned int tn = (t != NONE && next_raw < num_tiles) ? next_raw : NONE;
+      s_ticket[(it + 1) & 1] = tn;
+      if (tn != NONE && tma_ok) {
+        if (issued_store) tma_store_wait_read();  // buffer bn (stored last iteration) free again
+        issued[bn] += scan_issue_tile_load(in, n, tn, buf0 + bn * TILE, &s_bar[bn], keep) ? 1u : 0u;
       }
+      next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
+    }
+
+    // ---- compute: phase 1 of t
+    T *const bT = buf0 + bt * TILE;
+    if (!tma_ok) {
+      if (compute && t != NONE) scan_sync_tile_load(in, n, t, bT);
+      if (compute) named_barrier_sync(2, 32 * kScanWarps);
+    }
+    if (compute && t != NONE) {
+      if (has_tma(t) && !mbar_wait(&s_bar[bt], parity[bt], spin_limit_ns)) {
+        record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
+        abort_now();
+      }
+      const uint32_t count = scan_tile_count<T>(n, t);
+      T a = Op::identity();
 #pragma unroll
       for (int k = 0; k < R; ++k) {
         const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
-        uint4 c = reinterpret_cast<const uint4 *>(bufB)[chunk];
-        memcpy(&y[k][0], &c, 16);
-        if (chunk * V + V > count) {
+        T x[V];
+        const uint4 c = reinterpret_cast<const uint4 *>(bT)[chunk];
+        memcpy(&x[0], &c, 16);
 #pragma unroll
-          for (int j = 0; j < V; ++j)
-            if (chunk * V + j >= count) y[k][j] = Op::identity();
-        }
-#pragma unroll
-        for (int j = 1; j < V; ++j) y[k][j] = op(y[k][j - 1], y[k][j]);
-        const T incl = warp_inclusive_scan(y[k][V - 1], op, lane);
-        const T excl = shfl_up(incl, 1);
-        const T row_total = shfl_idx_any(incl, 31);
-        if (lane == 0) {
-          if (have) {
-#pragma unroll
-            for (int j = 0; j < V; ++j) y[k][j] = op(carry, y[k][j]);
-          }
-        } else {
-          const T pre = have ? op(carry, excl) : excl;
-#pragma unroll
-          for (int j = 0; j < V; ++j) y[k][j] = op(pre, y[k][j]);
-        }
-        carry = have ? op(carry, row_total) : row_total;
-        have = true;
+        for (int j = 0; j < V; ++j)
+          if (chunk * V + j < count) a = op(a, x[j]);
       }
+      a = warp_reduce(a, op);
+      if (lane == 0) s_wtot[it & 3][warp] = a;
     }
-    __syncthreads();
-    if (s_abort) break;
+    if (has_tma(t)) parity[bt] ^= 1u;
+    if (tid == 0) s_abort_seen[(2 * it) & 3] = aborted() ? 1 : 0;
+    named_barrier_sync(1, kScanMainThreads);
+    if (s_abort_seen[(2 * it) & 3]) break;
 
-    if (pending != NONE) {
-      const uint32_t count = scan_tile_count<T>(n, pending);
-      const uint64_t base = (uint64_t)pending * TILE;
-      if (!control) {
-        // ---- add the tile's exclusive prefix, back to shared memory
-        const T prefix = s_prefix;
+    // ---- thread 0: publish t's aggregate and queue t for the look-back
+    if (tid == 0) {
+      T agg = Op::identity();
+      if (t != NONE) {
+        agg = s_wtot[it & 3][0];
+#pragma unroll
+        for (int i = 1; i < kScanWarps; ++i) agg = op(agg, s_wtot[it & 3][i]);
+        if ((long long)t != skip_publish_tile) {
+          if (t == 0) st.publish(0u, kStPrefix, op(init, agg));
+          else st.publish(t, kStAggregate, agg);
+        }
+      }
+      s_q_tile[it % Q] = t;
+      s_q_agg[it % Q] = agg;
+      st_release_cta_u32(&s_q_in, (unsigned int)it + 1u);
+    }
+    // ---- loader: re-read t_{i-1} from L2 into t's buffer (phase 1 of t is done)
+    if (leader && q_tile != NONE && tma_ok)
+      issued[bt] += scan_issue_tile_load(in, n, q_tile, bT, &s_bar[bt], stream) ? 1u : 0u;
+
+    // ---- compute: phase 2 of p
+    if (compute && p != NONE) {
+      const uint32_t count = scan_tile_count<T>(n, p);
+      const uint64_t base = (uint64_t)p * TILE;
+      T *const bP = buf0 + bp * TILE;
+      // p's exclusive prefix: queue entry it - 2
+      const unsigned int e = (unsigned int)it - 2u;
+      bool ok = true;
+      unsigned long long w0 = 0;
+      for (unsigned int spins = 0; ld_acquire_cta_u32(&s_q_out) <= e; ++spins) {
+        if (aborted()) {
+          ok = false;
+          break;
+        }
+        if ((spins & 15u) == 15u) {
+          const unsigned long long now = globaltimer_ns();
+          if (w0 == 0) w0 = now;
+          else if (now - w0 > spin_limit_ns) {
+            record_error(hdr, BK_ERR_SPIN_TIMEOUT, p);
+            abort_now();
+            ok = false;
+            break;
+          }
+        }
+        __nanosleep(32);
+      }
+      if (has_tma(p)) {
+        if (!mbar_wait(&s_bar[bp], parity[bp], spin_limit_ns)) {
+          record_error(hdr, BK_ERR_SPIN_TIMEOUT, p);
+          abort_now();
+          ok = false;
+        }
+      }
+      if (ok) {
+        T before = s_q_prefix[e % Q];  // everything before this warp's first element
+        for (int i = 0; i < warp; ++i) before = op(before, s_wtot[(it + 2) & 3][i]);
+        T y[R][V], incl[R];
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-          const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
+          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+          if (tma_ok) {
+            const uint4 c = reinterpret_cast<const uint4 *>(bP)[elem / V];
+            memcpy(&y[k][0], &c, 16);
+          } else {
 #pragma unroll
-          for (int j = 0; j < V; ++j) y[k][j] = op(prefix, y[k][j]);
-          uint4 c;
-          memcpy(&c, &y[k][0], 16);
-          reinterpret_cast<uint4 *>(bufB)[chunk] = c;
+            for (int j = 0; j < V; ++j) y[k][j] = (elem + j < count) ? in[base + elem + j] : Op::identity();
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+          if (elem + V > count) {
+#pragma unroll
+            for (int j = 0; j < V; ++j)
+              if (elem + j >= count) y[k][j] = Op::identity();
+          }
+#pragma unroll
+          for (int j = 1; j < V; ++j) y[k][j] = op(y[k][j - 1], y[k][j]);
+          incl[k] = y[k][V - 1];
+        }
+        // the rows' warp scans, interleaved so their shuffle chains overlap
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+          for (int k = 0; k < R; ++k) {
+            const T o = shfl_up(incl[k], d);
+            if (lane >= d) incl[k] = op(o, incl[k]);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const T ex = shfl_up(incl[k], 1);
+          const T tot = shfl_idx_any(incl[k], 31);
+          const T b = lane != 0 ? op(before, ex) : before;
+#pragma unroll
+          for (int j = 0; j < V; ++j) y[k][j] = op(b, y[k][j]);
+          before = op(before, tot);
+          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+          if (tma_ok) {
+            uint4 c;
+            memcpy(&c, &y[k][0], 16);
+            reinterpret_cast<uint4 *>(bP)[elem / V] = c;
+          } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j)
+              if (elem + j < count) out[base + elem + j] = y[k][j];
+          }
         }
         if (tma_ok) fence_proxy_async_smem();
       }
-      __syncthreads();
-      if (tma_ok) {
-        if (leader) {
-          const uint32_t bulk = count & ~(uint32_t)(V - 1);
-          if (bulk > 0) {
-            tma_store_1d_hint(out + base, bufB, bulk * (uint32_t)sizeof(T), stream);
-            tma_store_commit();
-            issued_store = true;
-          }
-          for (uint32_t i = bulk; i < count; ++i) out[base + i] = bufB[i];
-        }
-      } else if (!control) {
-        for (uint32_t i = tid; i < count; i += kScanWarps * 32) out[base + i] = bufB[i];
+    }
+    if (has_tma(p)) parity[bp] ^= 1u;
+    if (tid == 0) s_abort_seen[(2 * it + 1) & 3] = aborted() ? 1 : 0;
+    named_barrier_sync(1, kScanMainThreads);
+    if (s_abort_seen[(2 * it + 1) & 3]) break;
+
+    // ---- loader: store p
+    if (leader && p != NONE && tma_ok) {
+      const uint32_t count = scan_tile_count<T>(n, p);
+      const uint64_t base = (uint64_t)p * TILE;
+      const T *bP = buf0 + bp * TILE;
+      const uint32_t bulk = count & ~(uint32_t)(V - 1);
+      if (bulk > 0) {
+        tma_store_1d_hint(out + base, bP, bulk * (uint32_t)sizeof(T), stream);
+        tma_store_commit();
+        issued_store = true;
       }
+      for (uint32_t i = bulk; i < count; ++i) out[base + i] = bP[i];
     }
 
-    if (t == NONE) break;  // nothing left: the pending tile was the last
-    pending = t;
-    pending_agg = agg_t;
-    __syncthreads();  // the non-TMA path's plain stores read bufB
+    p_tile = q_tile;
+    q_tile = t;
+    if (t == NONE && p_tile == NONE && q_tile == NONE) break;  // tickets only grow: nothing left
   }
 
-  // Drain: every bulk store must finish reading shared memory, and on an
-  // abort every prefetch must land, before the CTA's shared memory goes away.
+  // Drain: every bulk store must finish reading shared memory, and every
+  // load must land (on an abort some were never waited for), before the
+  // CTA's shared memory goes away.  Each barrier has at most one load
+  // outstanding, the last one issued; waiting for a phase that already
+  // completed returns at once.
   if (leader) {
     if (issued_store) tma_store_wait_all();
-    for (int b = 0; b < 3; ++b)
-      if (inflight & (1u << b)) (void)mbar_wait(&s_bar[b], parity[b], spin_limit_ns);
+    for (int b = 0; b < NB; ++b)
+      if (issued[b] != 0u) (void)mbar_wait(&s_bar[b], (issued[b] - 1u) & 1u, spin_limit_ns);
   }
 }
 
@@ -374,7 +462,7 @@ int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t 
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
   const int tma_ok = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15) == 0;
-  const size_t smem = 3 * (size_t)C::TILE_BYTES;
+  const size_t smem = (size_t)kScanBufs * C::TILE_BYTES;
   static thread_local bool attr_set = false;  // per host thread; cheap and idempotent
   if (!attr_set) {
     if ((st = host::set_smem_attrs(scan_kernel<T, Op>, smem)) != BK_OK) return st;
