@@ -23,11 +23,10 @@
 
 namespace bk {
 
-constexpr int kScanWarps = 8;                                // compute warps (0-7)
-constexpr int kScanMainThreads = 32 * (kScanWarps + 1);      // + the loader warp (8): barrier 1
-constexpr int kScanThreads = kScanMainThreads + 32;          // + the look-back warp (9)
+constexpr int kScanWarps = 8;                        // compute warps (0-7)
+constexpr int kScanThreads = 32 * (kScanWarps + 2);  // + the loader warp (8; one lane works) + the look-back warp (9)
 constexpr int kScanRowsPerWarp = 8;
-constexpr int kScanBufs = 3;  // tile buffers in rotation (see scan_kernel)
+constexpr int kScanBufs = 3;   // tile buffers in rotation (see scan_kernel)
 constexpr int kScanQueue = 4;  // look-back queue entries (more than the 2-iteration lag)
 
 template <typename T>
@@ -114,19 +113,26 @@ __device__ __forceinline__ uint32_t scan_tile_count(uint64_t n, unsigned int til
 //                  (evict-first), after which the buffer takes the prefetch
 //                  of t_{i+2}.
 // So every TMA load is issued about an iteration before it is needed, and a
-// tile's data waits in L2, not shared memory, between its two phases.  The
-// look-back warp runs beside all this on its own: it takes queued tiles in
-// order, each one once the next has been queued (its predecessors have then
-// had an iteration to publish), and hands back the exclusive prefix through
-// a shared-memory queue two iterations after the tile's phase 1.  The compute
-// and loader warps meet at two named barriers per iteration; the look-back
-// warp meets nobody, so its L2 round trips are off their critical path.
-// Whether a tile has a TMA copy depends only on (tile, n, alignment), so
-// every thread tracks the mbarrier phases itself.  Every look-back wait
-// points at a lower tile whose ticket a running CTA already took and whose
-// aggregate depends only on its load, so the waits always end; every wait
-// (look-back, mbarrier, queue) is still bounded by spin_limit_ns, and a
-// failure anywhere stops the CTA at its next barrier.
+// tile's data waits in L2, not shared memory, between its two phases.
+//
+// The three roles never share a barrier: they hand over through mbarriers.
+// full[b]: the loader completes one phase per use of buffer b (a TMA copy,
+// or a plain arrival when there is nothing to copy), after writing the
+// buffer's ticket, so the compute warps learn the ticket by waiting on it;
+// p1[b] / p2[b]: each compute warp arrives when it has finished reading
+// (phase 1) or writing (phase 2) buffer b, which is when the loader may reuse
+// it; qbar[e]: the look-back warp hands over queue entry e's exclusive
+// prefix.  Consecutive phases of one barrier are three iterations apart and
+// each waits on the previous one's data, so they cannot alias.  The compute
+// warps meet only each other, once per iteration (the warp totals), in a
+// barrier that also ORs their failure flags, so they all stop together.
+// The look-back warp takes queued tiles in order, each once the next one is
+// queued (its predecessors have then had an iteration to publish), so its L2
+// round trips are off everyone's critical path.  Every look-back wait points
+// at a lower tile whose ticket a running CTA already took and whose aggregate
+// depends only on its load and on a look-back for a still lower tile, so the
+// waits always end; every wait is still bounded by spin_limit_ns and gives up
+// at once when anyone in the CTA has failed.
 template <typename T, typename Op>
 __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *out, uint64_t n, T init,
                                                                typename ScanCfg<T>::Status st, WsHeader *hdr,
@@ -139,53 +145,134 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
   Op op;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T *const buf0 = reinterpret_cast<T *>(smem_raw);  // NB tile buffers
-  __shared__ __align__(8) uint64_t s_bar[NB];
-  __shared__ unsigned int s_ticket[2];   // t_i, by iteration parity
+  __shared__ __align__(8) uint64_t s_full[NB];
+  __shared__ __align__(8) uint64_t s_p1[NB];
+  __shared__ __align__(8) uint64_t s_p2[NB];
+  __shared__ __align__(8) uint64_t s_qbar[Q];
+  __shared__ unsigned int s_ticket[NB];  // ticket of the tile prefetched into buffer b
   __shared__ T s_wtot[4][kScanWarps];    // per-warp totals of t_i, by iteration mod 4
   __shared__ unsigned int s_q_tile[Q];   // look-back queue: entry j = t_j
   __shared__ T s_q_agg[Q];
   __shared__ T s_q_prefix[Q];
-  __shared__ unsigned int s_q_in, s_q_out;  // entries queued / prefixes returned
+  __shared__ unsigned int s_q_in;        // entries queued
   __shared__ int s_abort;
-  __shared__ int s_abort_seen[4];        // s_abort as tid 0 saw it before each barrier 1 (two per iteration)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const bool compute = warp < kScanWarps;
-  const bool loader_warp = warp == kScanWarps;
-  const bool leader = loader_warp && lane == 0;
-  const bool lbwarp = warp == kScanWarps + 1;
   // a TMA copy exists for `tile` exactly when this holds (scan_issue_tile_load)
   auto has_tma = [&](unsigned int tile) -> bool {
     return tma_ok && tile != NONE && (scan_tile_count<T>(n, tile) & ~(uint32_t)(V - 1)) != 0u;
   };
   auto abort_now = [&]() { *reinterpret_cast<volatile int *>(&s_abort) = 1; };
   auto aborted = [&]() -> bool { return *reinterpret_cast<volatile int *>(&s_abort) != 0; };
+  auto buf = [&](int b) { return buf0 + b * TILE; };
 
-  unsigned int next_raw = NONE;  // loader: next ticket, not yet range-checked
-  bool issued_store = false;     // loader
-  uint32_t issued[NB];           // loader: TMA loads issued on each of s_bar[]
-#pragma unroll
-  for (int b = 0; b < NB; ++b) issued[b] = 0u;
   uint64_t keep = 0, stream = 0;
-  if (leader) {
+  uint32_t armed[NB];  // loader: phases armed on s_full[b]
+#pragma unroll
+  for (int b = 0; b < NB; ++b) armed[b] = 0u;
+  unsigned int next_raw = NONE;  // loader: next ticket, not yet range-checked
+  unsigned int t_first = NONE;   // loader: t_0
+  if (tid == 32 * kScanWarps) {
     keep = l2_policy_evict_last();
     stream = l2_policy_evict_first();
-    for (int b = 0; b < NB; ++b) mbar_init(&s_bar[b], 1);
+    for (int b = 0; b < NB; ++b) {
+      mbar_init(&s_full[b], 1);
+      mbar_init(&s_p1[b], kScanWarps);
+      mbar_init(&s_p2[b], kScanWarps);
+    }
+    for (int q = 0; q < Q; ++q) mbar_init(&s_qbar[q], 1);
     fence_proxy_async_smem();
     s_abort = 0;
     s_q_in = 0u;
-    s_q_out = 0u;
     const unsigned int t0 = atomicAdd(&hdr->tile_ticket, 1u);
-    s_ticket[0] = t0 < num_tiles ? t0 : NONE;
-    if (t0 < num_tiles) {
-      if (tma_ok) issued[0] += scan_issue_tile_load(in, n, t0, buf0, &s_bar[0], keep) ? 1u : 0u;
-      next_raw = atomicAdd(&hdr->tile_ticket, 1u);
-    }
+    t_first = t0 < num_tiles ? t0 : NONE;
+    s_ticket[0] = t_first;
+    bool tx = false;
+    if (t_first != NONE && tma_ok) tx = scan_issue_tile_load(in, n, t_first, buf(0), &s_full[0], keep);
+    if (!tx) mbar_arrive(&s_full[0]);
+    armed[0] = 1u;
+    // iteration 0's phase 2 reads buffer NB - 1, which no re-read filled:
+    // give it an empty phase
+    mbar_arrive(&s_full[NB - 1]);
+    armed[NB - 1] = 1u;
+    if (t_first != NONE) next_raw = atomicAdd(&hdr->tile_ticket, 1u);
   }
   __syncthreads();
 
-  if (lbwarp) {
-    // ---- the look-back warp.  Waits (bounded) until `count` entries are
-    // queued; false on an abort or a timeout.
+  if (warp == kScanWarps) {
+    // ================= the loader (lane 0) =================
+    if (lane != 0) return;
+    uint32_t p1par[NB], p2par[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) p1par[b] = p2par[b] = 0u;
+    bool issued_store = false;
+    unsigned int t = t_first, p_tile = NONE, q_tile = NONE;
+    for (int it = 0;; ++it) {
+      const int bt = it % NB, bp = (it + NB - 1) % NB, bn = (it + 1) % NB;
+      const unsigned int p = p_tile;
+      // prefetch t_{i+1} into bn (stored last iteration), take the ticket after that
+      const unsigned int tn = (t != NONE && next_raw < num_tiles) ? next_raw : NONE;
+      s_ticket[bn] = tn;
+      bool tx = false;
+      if (tn != NONE && tma_ok) {
+        if (issued_store) tma_store_wait_read();
+        tx = scan_issue_tile_load(in, n, tn, buf(bn), &s_full[bn], keep);
+      }
+      if (!tx) mbar_arrive(&s_full[bn]);
+      ++armed[bn];
+      next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
+      // once the compute warps are done with buffer bt (phase 1 of t, or
+      // just its empty phase), re-read t_{i-1} from L2 into it
+      if (!mbar_wait_or_abort(&s_p1[bt], p1par[bt], spin_limit_ns, &s_abort)) {
+        record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
+        abort_now();
+        break;
+      }
+      p1par[bt] ^= 1u;
+      tx = false;
+      if (q_tile != NONE && tma_ok) tx = scan_issue_tile_load(in, n, q_tile, buf(bt), &s_full[bt], stream);
+      if (!tx) mbar_arrive(&s_full[bt]);
+      ++armed[bt];
+      // once the compute warps are done with buffer bp (phase 2 of p, or just
+      // its empty phase), store p; the buffer then takes the next prefetch
+      if (!mbar_wait_or_abort(&s_p2[bp], p2par[bp], spin_limit_ns, &s_abort)) {
+        record_error(hdr, BK_ERR_SPIN_TIMEOUT, p);
+        abort_now();
+        break;
+      }
+      p2par[bp] ^= 1u;
+      if (p != NONE) {
+        if (tma_ok) {
+          const uint32_t count = scan_tile_count<T>(n, p);
+          const uint64_t base = (uint64_t)p * TILE;
+          const T *bP = buf(bp);
+          const uint32_t bulk = count & ~(uint32_t)(V - 1);
+          if (bulk > 0) {
+            tma_store_1d_hint(out + base, bP, bulk * (uint32_t)sizeof(T), stream);
+            tma_store_commit();
+            issued_store = true;
+          }
+          for (uint32_t i = bulk; i < count; ++i) out[base + i] = bP[i];
+        }
+      }
+      p_tile = q_tile;
+      q_tile = t;
+      t = tn;
+      if (t == NONE && p_tile == NONE && q_tile == NONE) break;  // tickets only grow: nothing left
+    }
+    // Drain: stores must finish reading shared memory and every load must
+    // land before the CTA's shared memory goes away.  Phases of a barrier
+    // complete in order, so waiting for the last one armed covers them all;
+    // a phase that already completed returns at once.
+    if (issued_store) tma_store_wait_all();
+    for (int b = 0; b < NB; ++b)
+      if (armed[b] != 0u) (void)mbar_wait(&s_full[b], (armed[b] - 1u) & 1u, spin_limit_ns);
+    return;
+  }
+
+  if (warp == kScanWarps + 1) {
+    // ================= the look-back warp =================
+    // Waits (bounded) until `count` entries are queued; false on an abort or
+    // a timeout.
     auto wait_queued = [&](unsigned int count) -> bool {
       unsigned long long w0 = 0;
       bool ready = false;
@@ -226,7 +313,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
         if (ok) {
           if (q != 0 && (long long)q != skip_publish_tile) st.publish(q, kStPrefix, op(excl, agg));
           s_q_prefix[j % Q] = excl;
-          st_release_cta_u32(&s_q_out, j + 1u);
+          mbar_arrive(&s_qbar[j % Q]);
         } else {
           abort_now();
         }
@@ -236,60 +323,52 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
     return;
   }
 
-  // ---- compute warps and the loader
-  uint32_t parity[NB];
+  // ================= the compute warps =================
+  uint32_t fpar[NB];
 #pragma unroll
-  for (int b = 0; b < NB; ++b) parity[b] = 0u;
+  for (int b = 0; b < NB; ++b) fpar[b] = 0u;
   unsigned int p_tile = NONE, q_tile = NONE;  // t_{i-2}, t_{i-1}
+  bool bad = false;                           // this thread saw a failure
 
   for (int it = 0;; ++it) {
-    const int bt = it % NB;              // buffer of t_i
-    const int bp = (it + NB - 1) % NB;   // buffer of p = t_{i-2}: re-read there last iteration
-    const int bn = (it + 1) % NB;        // buffer for the prefetch of t_{i+1}
-    const unsigned int t = s_ticket[it & 1];
+    const int bt = it % NB, bp = (it + NB - 1) % NB;
     const unsigned int p = p_tile;
 
-    // ---- loader: prefetch t_{i+1} into the buffer whose store went out last
-    if (leader) {
-      const unsigned int tn = (t != NONE && next_raw < num_tiles) ? next_raw : NONE;
-      s_ticket[(it + 1) & 1] = tn;
-      if (tn != NONE && tma_ok) {
-        if (issued_store) tma_store_wait_read();  // buffer bn (stored last iteration) free again
-        issued[bn] += scan_issue_tile_load(in, n, tn, buf0 + bn * TILE, &s_bar[bn], keep) ? 1u : 0u;
-      }
-      next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
-    }
-
-    // ---- compute: phase 1 of t
-    T *const bT = buf0 + bt * TILE;
-    if (!tma_ok) {
-      if (compute && t != NONE) scan_sync_tile_load(in, n, t, bT);
-      if (compute) named_barrier_sync(2, 32 * kScanWarps);
-    }
-    if (compute && t != NONE) {
-      if (has_tma(t) && !mbar_wait(&s_bar[bt], parity[bt], spin_limit_ns)) {
-        record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
-        abort_now();
-      }
+    // ---- phase 1 of t: wait for buffer bt, learn t
+    unsigned int t = NONE;
+    if (!mbar_wait_or_abort(&s_full[bt], fpar[bt], spin_limit_ns, &s_abort)) bad = true;
+    fpar[bt] ^= 1u;
+    bad = __any_sync(0xffffffffu, bad);  // warp-uniform, so the shuffles below never diverge
+    if (!bad) t = s_ticket[bt];
+    if (t != NONE) {
       const uint32_t count = scan_tile_count<T>(n, t);
+      const uint64_t base = (uint64_t)t * TILE;
+      const T *bT = buf(bt);
       T a = Op::identity();
 #pragma unroll
       for (int k = 0; k < R; ++k) {
-        const uint32_t chunk = (uint32_t)((warp * R + k) * 32 + lane);
+        const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
         T x[V];
-        const uint4 c = reinterpret_cast<const uint4 *>(bT)[chunk];
-        memcpy(&x[0], &c, 16);
+        if (tma_ok) {
+          const uint4 c = reinterpret_cast<const uint4 *>(bT)[elem / V];
+          memcpy(&x[0], &c, 16);
+        } else {
+#pragma unroll
+          for (int j = 0; j < V; ++j) x[j] = (elem + j < count) ? in[base + elem + j] : Op::identity();
+        }
 #pragma unroll
         for (int j = 0; j < V; ++j)
-          if (chunk * V + j < count) a = op(a, x[j]);
+          if (elem + j < count) a = op(a, x[j]);
       }
       a = warp_reduce(a, op);
       if (lane == 0) s_wtot[it & 3][warp] = a;
     }
-    if (has_tma(t)) parity[bt] ^= 1u;
-    if (tid == 0) s_abort_seen[(2 * it) & 3] = aborted() ? 1 : 0;
-    named_barrier_sync(1, kScanMainThreads);
-    if (s_abort_seen[(2 * it) & 3]) break;
+    // done with buffer bt (also when it held nothing); after a failure the
+    // loader is told nothing more -- it gives up on the abort flag instead
+    __syncwarp();
+    if (!bad && lane == 0) mbar_arrive(&s_p1[bt]);
+    if (named_barrier_or(1, 32 * kScanWarps, bad || aborted())) break;
+    // no thread failed before this barrier, so t is the same everywhere
 
     // ---- thread 0: publish t's aggregate and queue t for the look-back
     if (tid == 0) {
@@ -307,134 +386,82 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
       s_q_agg[it % Q] = agg;
       st_release_cta_u32(&s_q_in, (unsigned int)it + 1u);
     }
-    // ---- loader: re-read t_{i-1} from L2 into t's buffer (phase 1 of t is done)
-    if (leader && q_tile != NONE && tma_ok)
-      issued[bt] += scan_issue_tile_load(in, n, q_tile, bT, &s_bar[bt], stream) ? 1u : 0u;
 
-    // ---- compute: phase 2 of p
-    if (compute && p != NONE) {
-      const uint32_t count = scan_tile_count<T>(n, p);
-      const uint64_t base = (uint64_t)p * TILE;
-      T *const bP = buf0 + bp * TILE;
-      // p's exclusive prefix: queue entry it - 2
+    // ---- phase 2 of p: buffer bp (re-read last iteration), prefix = queue entry it - 2
+    if (!mbar_wait_or_abort(&s_full[bp], fpar[bp], spin_limit_ns, &s_abort)) bad = true;
+    fpar[bp] ^= 1u;
+    if (p != NONE && !bad) {
       const unsigned int e = (unsigned int)it - 2u;
-      bool ok = true;
-      unsigned long long w0 = 0;
-      for (unsigned int spins = 0; ld_acquire_cta_u32(&s_q_out) <= e; ++spins) {
-        if (aborted()) {
-          ok = false;
-          break;
-        }
-        if ((spins & 15u) == 15u) {
-          const unsigned long long now = globaltimer_ns();
-          if (w0 == 0) w0 = now;
-          else if (now - w0 > spin_limit_ns) {
-            record_error(hdr, BK_ERR_SPIN_TIMEOUT, p);
-            abort_now();
-            ok = false;
-            break;
-          }
-        }
-        __nanosleep(32);
-      }
-      if (has_tma(p)) {
-        if (!mbar_wait(&s_bar[bp], parity[bp], spin_limit_ns)) {
-          record_error(hdr, BK_ERR_SPIN_TIMEOUT, p);
-          abort_now();
-          ok = false;
-        }
-      }
-      if (ok) {
-        T before = s_q_prefix[e % Q];  // everything before this warp's first element
-        for (int i = 0; i < warp; ++i) before = op(before, s_wtot[(it + 2) & 3][i]);
-        T y[R][V], incl[R];
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
-          if (tma_ok) {
-            const uint4 c = reinterpret_cast<const uint4 *>(bP)[elem / V];
-            memcpy(&y[k][0], &c, 16);
-          } else {
-#pragma unroll
-            for (int j = 0; j < V; ++j) y[k][j] = (elem + j < count) ? in[base + elem + j] : Op::identity();
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
-          if (elem + V > count) {
-#pragma unroll
-            for (int j = 0; j < V; ++j)
-              if (elem + j >= count) y[k][j] = Op::identity();
-          }
-#pragma unroll
-          for (int j = 1; j < V; ++j) y[k][j] = op(y[k][j - 1], y[k][j]);
-          incl[k] = y[k][V - 1];
-        }
-        // the rows' warp scans, interleaved so their shuffle chains overlap
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-#pragma unroll
-          for (int k = 0; k < R; ++k) {
-            const T o = shfl_up(incl[k], d);
-            if (lane >= d) incl[k] = op(o, incl[k]);
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const T ex = shfl_up(incl[k], 1);
-          const T tot = shfl_idx_any(incl[k], 31);
-          const T b = lane != 0 ? op(before, ex) : before;
-#pragma unroll
-          for (int j = 0; j < V; ++j) y[k][j] = op(b, y[k][j]);
-          before = op(before, tot);
-          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
-          if (tma_ok) {
-            uint4 c;
-            memcpy(&c, &y[k][0], 16);
-            reinterpret_cast<uint4 *>(bP)[elem / V] = c;
-          } else {
-#pragma unroll
-            for (int j = 0; j < V; ++j)
-              if (elem + j < count) out[base + elem + j] = y[k][j];
-          }
-        }
-        if (tma_ok) fence_proxy_async_smem();
-      }
+      if (!mbar_wait_or_abort(&s_qbar[e % Q], (e / Q) & 1u, spin_limit_ns, &s_abort)) bad = true;
     }
-    if (has_tma(p)) parity[bp] ^= 1u;
-    if (tid == 0) s_abort_seen[(2 * it + 1) & 3] = aborted() ? 1 : 0;
-    named_barrier_sync(1, kScanMainThreads);
-    if (s_abort_seen[(2 * it + 1) & 3]) break;
-
-    // ---- loader: store p
-    if (leader && p != NONE && tma_ok) {
+    bad = __any_sync(0xffffffffu, bad);
+    if (p != NONE && !bad) {
       const uint32_t count = scan_tile_count<T>(n, p);
       const uint64_t base = (uint64_t)p * TILE;
-      const T *bP = buf0 + bp * TILE;
-      const uint32_t bulk = count & ~(uint32_t)(V - 1);
-      if (bulk > 0) {
-        tma_store_1d_hint(out + base, bP, bulk * (uint32_t)sizeof(T), stream);
-        tma_store_commit();
-        issued_store = true;
+      T *const bP = buf(bp);
+      const unsigned int e = (unsigned int)it - 2u;
+      T before = s_q_prefix[e % Q];  // everything before this warp's first element
+      for (int i = 0; i < warp; ++i) before = op(before, s_wtot[(it + 2) & 3][i]);
+      T y[R][V], incl[R];
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+        if (tma_ok) {
+          const uint4 c = reinterpret_cast<const uint4 *>(bP)[elem / V];
+          memcpy(&y[k][0], &c, 16);
+        } else {
+#pragma unroll
+          for (int j = 0; j < V; ++j) y[k][j] = (elem + j < count) ? in[base + elem + j] : Op::identity();
+        }
       }
-      for (uint32_t i = bulk; i < count; ++i) out[base + i] = bP[i];
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+        if (elem + V > count) {
+#pragma unroll
+          for (int j = 0; j < V; ++j)
+            if (elem + j >= count) y[k][j] = Op::identity();
+        }
+#pragma unroll
+        for (int j = 1; j < V; ++j) y[k][j] = op(y[k][j - 1], y[k][j]);
+        incl[k] = y[k][V - 1];
+      }
+      // the rows' warp scans, interleaved so their shuffle chains overlap
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const T o = shfl_up(incl[k], d);
+          if (lane >= d) incl[k] = op(o, incl[k]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const T ex = shfl_up(incl[k], 1);
+        const T tot = shfl_idx_any(incl[k], 31);
+        const T b = lane != 0 ? op(before, ex) : before;
+#pragma unroll
+        for (int j = 0; j < V; ++j) y[k][j] = op(b, y[k][j]);
+        before = op(before, tot);
+        const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+        if (tma_ok) {
+          uint4 c;
+          memcpy(&c, &y[k][0], 16);
+          reinterpret_cast<uint4 *>(bP)[elem / V] = c;
+        } else {
+#pragma unroll
+          for (int j = 0; j < V; ++j)
+            if (elem + j < count) out[base + elem + j] = y[k][j];
+        }
+      }
+      if (tma_ok) fence_proxy_async_smem();
     }
+    __syncwarp();
+    if (!bad && lane == 0) mbar_arrive(&s_p2[bp]);
 
     p_tile = q_tile;
     q_tile = t;
     if (t == NONE && p_tile == NONE && q_tile == NONE) break;  // tickets only grow: nothing left
-  }
-
-  // Drain: every bulk store must finish reading shared memory, and every
-  // load must land (on an abort some were never waited for), before the
-  // CTA's shared memory goes away.  Each barrier has at most one load
-  // outstanding, the last one issued; waiting for a phase that already
-  // completed returns at once.
-  if (leader) {
-    if (issued_store) tma_store_wait_all();
-    for (int b = 0; b < NB; ++b)
-      if (issued[b] != 0u) (void)mbar_wait(&s_bar[b], (issued[b] - 1u) & 1u, spin_limit_ns);
   }
 }
 
