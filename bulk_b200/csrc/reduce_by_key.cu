@@ -16,9 +16,11 @@
 // (c1 + c2, c2 ? v2 : v1 + v2) is associative but not commutative, so every
 // fold keeps data order.  At each tail (last element of a run) the inclusive
 // (c, v) gives the run's output slot c - 1 and its sum v.  The tile pipeline
-// is the scan's (scan.cu): persistent CTAs with a control warp, TMA bulk tile
-// loads (keys and values) plus a one-key halo on each side, phase 1 publishes
-// the tile aggregate, phase 2 looks back and emits the tile's runs.
+// is the scan's (scan.cu): persistent CTAs whose compute warps, loader lane
+// and look-back warp hand over through mbarriers; three tile buffers rotate
+// through prefetch (keys, values and a one-key halo on each side, by TMA),
+// phase 1 (the tile aggregate, published), a re-read from L2 and phase 2
+// (the tile's runs, emitted once the look-back warp has found the prefix).
 #include "bk_common.cuh"
 #include "bk_lookback.cuh"
 #include "bk_tma.cuh"
@@ -42,8 +44,10 @@ struct OpSeg {
   __host__ __device__ static constexpr Seg<V> identity() { return Seg<V>{0u, V(0)}; }
 };
 
-constexpr int kRbkWarps = 8;
-constexpr int kRbkThreads = 32 * (kRbkWarps + 1);  // + control warp
+constexpr int kRbkWarps = 8;                       // compute warps (0-7)
+constexpr int kRbkThreads = 32 * (kRbkWarps + 2);  // + the loader warp (8; one lane works) + the look-back warp (9)
+constexpr int kRbkBufs = 3;                        // tile buffers in rotation (as in scan.cu)
+constexpr int kRbkQueue = 4;                       // look-back queue entries
 
 template <typename K, typename V>
 struct RbkCfg {
@@ -230,6 +234,13 @@ __device__ __forceinline__ Seg<V> lane_fold(const LaneRun<K, V, M> &lr) {
   return Seg<V>{c, v};
 }
 
+// Persistent two-phase reduce_by_key; the roles, buffer rotation and
+// hand-over protocol are scan_kernel's (scan.cu), with these differences: a
+// buffer holds a tile's keys, values and halo keys; phase 2 only reads its
+// buffer (the runs go straight to out_keys / out_vals), so the loader reuses
+// a buffer once the compute warps are done reading it, with no store to
+// drain; and without TMA (pointers not 16-byte aligned) the compute warps
+// stage both tiles themselves between two compute-only barriers.
 template <typename K, typename V>
 __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, const V *vals, uint64_t n, K *out_keys,
                                                              V *out_vals, uint64_t *d_num_out,
@@ -239,151 +250,223 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
                                                              unsigned int num_tiles) {
   using C = RbkCfg<K, V>;
   using P = typename C::P;
-  constexpr int M = C::M, TILE = C::TILE;
+  constexpr int M = C::M, TILE = C::TILE, NB = kRbkBufs, Q = kRbkQueue;
   constexpr unsigned int NONE = 0xffffffffu;
   OpSeg<V> op;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  unsigned char *const buf[3] = {smem_raw, smem_raw + C::BUF_BYTES, smem_raw + 2 * C::BUF_BYTES};
-  __shared__ __align__(8) uint64_t s_bar[3];
-  __shared__ __align__(16) K s_halo[3][2][16 / sizeof(K)];
-  __shared__ unsigned int s_ticket[2];
-  __shared__ int s_has_tma[3];
-  __shared__ P s_wagg[2][kRbkWarps];
-  __shared__ P s_prefix;
+  __shared__ __align__(16) K s_halo[NB][2][16 / sizeof(K)];
+  __shared__ __align__(8) uint64_t s_full[NB];
+  __shared__ __align__(8) uint64_t s_p1[NB];
+  __shared__ __align__(8) uint64_t s_p2[NB];
+  __shared__ __align__(8) uint64_t s_qbar[Q];
+  __shared__ unsigned int s_ticket[NB];
+  __shared__ P s_wagg[4][kRbkWarps];  // per-warp (c, v) of t_i, by iteration mod 4
+  __shared__ unsigned int s_q_tile[Q];
+  __shared__ P s_q_agg[Q];
+  __shared__ P s_q_prefix[Q];
+  __shared__ unsigned int s_q_in;
   __shared__ int s_abort;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const bool control = (warp == kRbkWarps);
-  const bool leader = control && lane == 0;
+  auto abort_now = [&]() { *reinterpret_cast<volatile int *>(&s_abort) = 1; };
+  auto aborted = [&]() -> bool { return *reinterpret_cast<volatile int *>(&s_abort) != 0; };
+  auto buf = [&](int b) { return smem_raw + (size_t)b * C::BUF_BYTES; };
+  auto tile_count = [&](unsigned int tile) -> uint32_t {
+    const uint64_t base = (uint64_t)tile * TILE;
+    return (uint32_t)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
+  };
 
-  unsigned int next_ticket = NONE;
   uint64_t keep = 0, stream = 0;
-  if (leader) {
+  uint32_t armed[NB];  // loader: phases armed on s_full[b]
+#pragma unroll
+  for (int b = 0; b < NB; ++b) armed[b] = 0u;
+  unsigned int next_raw = NONE;
+  unsigned int t_first = NONE;
+  if (tid == 32 * kRbkWarps) {
     keep = l2_policy_evict_last();
     stream = l2_policy_evict_first();
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
-    mbar_init(&s_bar[2], 1);
+    for (int b = 0; b < NB; ++b) {
+      mbar_init(&s_full[b], 1);
+      mbar_init(&s_p1[b], kRbkWarps);
+      mbar_init(&s_p2[b], kRbkWarps);
+    }
+    for (int q = 0; q < Q; ++q) mbar_init(&s_qbar[q], 1);
     fence_proxy_async_smem();
     s_abort = 0;
-    s_has_tma[0] = s_has_tma[1] = s_has_tma[2] = 0;
+    s_q_in = 0u;
     const unsigned int t0 = atomicAdd(&hdr->tile_ticket, 1u);
-    s_ticket[0] = t0 < num_tiles ? t0 : NONE;
-    if (t0 < num_tiles) {
-      s_has_tma[0] = rbk_issue_load<K, V>(keys, vals, n, t0, buf[0], s_halo[0], &s_bar[0], keep, tma_ok);
-      const unsigned int t1 = atomicAdd(&hdr->tile_ticket, 1u);
-      next_ticket = t1 < num_tiles ? t1 : NONE;
-    }
+    t_first = t0 < num_tiles ? t0 : NONE;
+    s_ticket[0] = t_first;
+    bool tx = false;
+    if (t_first != NONE) tx = rbk_issue_load<K, V>(keys, vals, n, t_first, buf(0), s_halo[0], &s_full[0], keep, tma_ok);
+    if (!tx) mbar_arrive(&s_full[0]);
+    armed[0] = 1u;
+    mbar_arrive(&s_full[NB - 1]);  // iteration 0's phase 2 reads buffer NB - 1: an empty phase
+    armed[NB - 1] = 1u;
+    if (t_first != NONE) next_raw = atomicAdd(&hdr->tile_ticket, 1u);
   }
   __syncthreads();
 
-  uint32_t parity[3] = {0u, 0u, 0u};
-  uint32_t inflight = s_has_tma[0] ? 1u : 0u;
-  unsigned int pending = NONE;
-  P pending_agg = OpSeg<V>::identity();
-
-  for (int it = 0;; ++it) {
-    const int slot = it & 1;
-    const unsigned int t = s_ticket[slot];
-
-    if (leader) {
-      s_has_tma[2] = 0;
-      if (pending != NONE)
-        s_has_tma[2] = rbk_issue_load<K, V>(keys, vals, n, pending, buf[2], s_halo[2], &s_bar[2], stream, tma_ok);
-      const unsigned int tn = (t != NONE) ? next_ticket : NONE;
-      s_ticket[slot ^ 1] = tn;
-      s_has_tma[slot ^ 1] = 0;
-      if (tn != NONE)
-        s_has_tma[slot ^ 1] =
-            rbk_issue_load<K, V>(keys, vals, n, tn, buf[slot ^ 1], s_halo[slot ^ 1], &s_bar[slot ^ 1], keep, tma_ok);
-      next_ticket = NONE;
-      if (tn != NONE) {
-        const unsigned int x = atomicAdd(&hdr->tile_ticket, 1u);
-        next_ticket = x < num_tiles ? x : NONE;
-      }
-    }
-    if (!tma_ok && !control) {
-      if (t != NONE) rbk_sync_load<K, V>(keys, vals, n, t, buf[slot]);
-      if (pending != NONE) rbk_sync_load<K, V>(keys, vals, n, pending, buf[2]);
-    }
-    __syncthreads();
-    if (s_has_tma[slot ^ 1]) inflight |= 1u << (slot ^ 1);
-    if (s_has_tma[2]) inflight |= 4u;
-
-    // ---- phase 1 of t: tile aggregate
-    if (t != NONE) {
-      if (inflight & (1u << slot)) {
-        if (!control && !mbar_wait(&s_bar[slot], parity[slot], spin_limit_ns)) {
-          record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
-          s_abort = 1;
-        }
-        parity[slot] ^= 1u;
-        inflight &= ~(1u << slot);
-      }
-      if (!control) {
-        const uint64_t base = (uint64_t)t * TILE;
-        const uint32_t count = (uint32_t)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
-        LaneRun<K, V, M> lr;
-        rbk_read_lane<K, V>(buf[slot], s_halo[slot], count, t == 0, base + count == n, warp, lane, lr);
-        const P incl = warp_inclusive_scan(lane_fold(lr), op, lane);
-        if (lane == 31) s_wagg[slot][warp] = incl;
-      }
-    }
-    __syncthreads();
-    P agg_t = OpSeg<V>::identity();
-    if (t != NONE) {
+  if (warp == kRbkWarps) {
+    // ================= the loader (lane 0) =================
+    if (lane != 0) return;
+    uint32_t p1par[NB], p2par[NB];
 #pragma unroll
-      for (int i = 0; i < kRbkWarps; ++i) agg_t = op(agg_t, s_wagg[slot][i]);
+    for (int b = 0; b < NB; ++b) p1par[b] = p2par[b] = 0u;
+    unsigned int t = t_first, p_tile = NONE, q_tile = NONE;
+    for (int it = 0;; ++it) {
+      const int bt = it % NB, bp = (it + NB - 1) % NB, bn = (it + 1) % NB;
+      // prefetch t_{i+1} into bn (the compute warps finished reading it last iteration)
+      const unsigned int tn = (t != NONE && next_raw < num_tiles) ? next_raw : NONE;
+      s_ticket[bn] = tn;
+      bool tx = false;
+      if (tn != NONE) tx = rbk_issue_load<K, V>(keys, vals, n, tn, buf(bn), s_halo[bn], &s_full[bn], keep, tma_ok);
+      if (!tx) mbar_arrive(&s_full[bn]);
+      ++armed[bn];
+      next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
+      // re-read t_{i-1} into t's buffer once phase 1 of t is done with it
+      if (!mbar_wait_or_abort(&s_p1[bt], p1par[bt], spin_limit_ns, &s_abort)) {
+        record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
+        abort_now();
+        break;
+      }
+      p1par[bt] ^= 1u;
+      tx = false;
+      if (q_tile != NONE)
+        tx = rbk_issue_load<K, V>(keys, vals, n, q_tile, buf(bt), s_halo[bt], &s_full[bt], stream, tma_ok);
+      if (!tx) mbar_arrive(&s_full[bt]);
+      ++armed[bt];
+      // buffer bp is free once phase 2 of p has read it
+      if (!mbar_wait_or_abort(&s_p2[bp], p2par[bp], spin_limit_ns, &s_abort)) {
+        record_error(hdr, BK_ERR_SPIN_TIMEOUT, p_tile);
+        abort_now();
+        break;
+      }
+      p2par[bp] ^= 1u;
+      p_tile = q_tile;
+      q_tile = t;
+      t = tn;
+      if (t == NONE && p_tile == NONE && q_tile == NONE) break;
     }
+    // every load must land before the CTA's shared memory goes away
+    for (int b = 0; b < NB; ++b)
+      if (armed[b] != 0u) (void)mbar_wait(&s_full[b], (armed[b] - 1u) & 1u, spin_limit_ns);
+    return;
+  }
 
-    LaneRun<K, V, M> lr2;                // phase-2 lane data, kept across the barrier
-    P lane_incl = OpSeg<V>::identity();  // its inclusive scan over the warp's lanes
-    if (control) {
-      if (leader && t != NONE && !s_abort && (long long)t != skip_publish_tile)
-        st.publish(t, t == 0 ? kStPrefix : kStAggregate, agg_t);
-      if (pending != NONE) {
-        const unsigned int p = pending;
-        P excl = OpSeg<V>::identity();
-        bool ok = true;
-        if (p != 0) ok = lookback_exclusive<P>(st, p, op, excl, hdr, spin_limit_ns);
-        if (leader) {
-          if (ok) {
-            if (p != 0 && (long long)p != skip_publish_tile) st.publish(p, kStPrefix, op(excl, pending_agg));
-            s_prefix = excl;
-          } else {
-            s_abort = 1;
+  if (warp == kRbkWarps + 1) {
+    // ================= the look-back warp =================
+    auto wait_queued = [&](unsigned int count) -> bool {
+      unsigned long long w0 = 0;
+      bool ready = false;
+      for (unsigned int spins = 0;; ++spins) {
+        if (ld_acquire_cta_u32(&s_q_in) >= count) {
+          ready = true;
+          break;
+        }
+        if (aborted()) break;
+        if ((spins & 15u) == 15u) {
+          const unsigned long long now = globaltimer_ns();
+          if (w0 == 0) w0 = now;
+          else if (now - w0 > spin_limit_ns) {
+            if (lane == 0) {
+              record_error(hdr, BK_ERR_SPIN_TIMEOUT, NONE);
+              abort_now();
+            }
+            break;
           }
         }
-        if (inflight & 4u) {
-          parity[2] ^= 1u;
-          inflight &= ~4u;
+        __nanosleep(64);
+      }
+      return __all_sync(0xffffffffu, ready);
+    };
+    for (unsigned int j = 0;; ++j) {
+      if (!wait_queued(j + 1u)) break;
+      const unsigned int q = s_q_tile[j % Q];
+      if (q == NONE) break;
+      if (!wait_queued(j + 2u)) break;
+      const P agg = s_q_agg[j % Q];
+      P excl = OpSeg<V>::identity();
+      bool ok = true;
+      if (q != 0) ok = lookback_exclusive<P>(st, q, op, excl, hdr, spin_limit_ns);
+      if (lane == 0) {
+        if (ok) {
+          if (q != 0 && (long long)q != skip_publish_tile) st.publish(q, kStPrefix, op(excl, agg));
+          s_q_prefix[j % Q] = excl;
+          mbar_arrive(&s_qbar[j % Q]);
+        } else {
+          abort_now();
         }
       }
-    } else if (pending != NONE) {
-      // phase 2, the part that needs no prefix: overlaps the look-back
-      if (inflight & 4u) {
-        if (!mbar_wait(&s_bar[2], parity[2], spin_limit_ns)) {
-          record_error(hdr, BK_ERR_SPIN_TIMEOUT, pending);
-          s_abort = 1;
-        }
-        parity[2] ^= 1u;
-        inflight &= ~4u;
-      }
-      const uint64_t base = (uint64_t)pending * TILE;
-      const uint32_t count = (uint32_t)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
-      rbk_read_lane<K, V>(buf[2], s_halo[2], count, pending == 0, base + count == n, warp, lane, lr2);
-      lane_incl = warp_inclusive_scan(lane_fold(lr2), op, lane);
+      if (!ok) break;
     }
-    __syncthreads();  // the prefix is known
-    if (s_abort) break;
+    return;
+  }
 
-    // ---- phase 2 of the pending tile: emit its runs
-    if (pending != NONE && !control) {
-      const uint64_t base = (uint64_t)pending * TILE;
-      const uint32_t count = (uint32_t)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
-      P carry = s_prefix;
-      for (int i = 0; i < warp; ++i) carry = op(carry, s_wagg[slot ^ 1][i]);
-      const bool last_tile = base + count == n;
-      const LaneRun<K, V, M> &lr = lr2;
+  // ================= the compute warps =================
+  uint32_t fpar[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) fpar[b] = 0u;
+  unsigned int p_tile = NONE, q_tile = NONE;
+  bool bad = false;
+
+  for (int it = 0;; ++it) {
+    const int bt = it % NB, bp = (it + NB - 1) % NB;
+    const unsigned int p = p_tile;
+
+    // ---- phase 1 of t
+    unsigned int t = NONE;
+    if (!mbar_wait_or_abort(&s_full[bt], fpar[bt], spin_limit_ns, &s_abort)) bad = true;
+    fpar[bt] ^= 1u;
+    bad = __any_sync(0xffffffffu, bad);
+    if (!bad) t = s_ticket[bt];
+    if (!tma_ok) {
+      // stage t and p here (previous iteration's readers are past the first barrier)
+      named_barrier_sync(2, 32 * kRbkWarps);
+      if (t != NONE) rbk_sync_load<K, V>(keys, vals, n, t, buf(bt));
+      if (p != NONE) rbk_sync_load<K, V>(keys, vals, n, p, buf(bp));
+      named_barrier_sync(2, 32 * kRbkWarps);
+    }
+    if (t != NONE) {
+      const uint32_t count = tile_count(t);
+      LaneRun<K, V, M> lr;
+      rbk_read_lane<K, V>(buf(bt), s_halo[bt], count, t == 0, (uint64_t)t * TILE + count == n, warp, lane, lr);
+      const P incl = warp_inclusive_scan(lane_fold(lr), op, lane);
+      if (lane == 31) s_wagg[it & 3][warp] = incl;
+    }
+    __syncwarp();
+    if (!bad && lane == 0) mbar_arrive(&s_p1[bt]);
+    if (named_barrier_or(1, 32 * kRbkWarps, bad || aborted())) break;
+
+    // ---- thread 0: publish t's aggregate and queue t for the look-back
+    if (tid == 0) {
+      P agg = OpSeg<V>::identity();
+      if (t != NONE) {
+#pragma unroll
+        for (int i = 0; i < kRbkWarps; ++i) agg = op(agg, s_wagg[it & 3][i]);
+        if ((long long)t != skip_publish_tile) st.publish(t, t == 0 ? kStPrefix : kStAggregate, agg);
+      }
+      s_q_tile[it % Q] = t;
+      s_q_agg[it % Q] = agg;
+      st_release_cta_u32(&s_q_in, (unsigned int)it + 1u);
+    }
+
+    // ---- phase 2 of p: emit its runs
+    if (!mbar_wait_or_abort(&s_full[bp], fpar[bp], spin_limit_ns, &s_abort)) bad = true;
+    fpar[bp] ^= 1u;
+    if (p != NONE && !bad) {
+      const unsigned int e = (unsigned int)it - 2u;
+      if (!mbar_wait_or_abort(&s_qbar[e % Q], (e / Q) & 1u, spin_limit_ns, &s_abort)) bad = true;
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (p != NONE && !bad) {
+      const unsigned int e = (unsigned int)it - 2u;
+      const uint32_t count = tile_count(p);
+      const bool last_tile = (uint64_t)p * TILE + count == n;
+      LaneRun<K, V, M> lr;
+      rbk_read_lane<K, V>(buf(bp), s_halo[bp], count, p == 0, last_tile, warp, lane, lr);
+      const P lane_incl = warp_inclusive_scan(lane_fold(lr), op, lane);
+      P carry = s_q_prefix[e % Q];
+      for (int i = 0; i < warp; ++i) carry = op(carry, s_wagg[(it + 2) & 3][i]);
       const P excl = shfl_up(lane_incl, 1);
       if (lane > 0) carry = op(carry, excl);
       // walk the lane's elements with the running (c, v); each tail emits its run
@@ -407,16 +490,12 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
         }
       }
     }
+    __syncwarp();
+    if (!bad && lane == 0) mbar_arrive(&s_p2[bp]);
 
-    if (t == NONE) break;
-    pending = t;
-    pending_agg = agg_t;
-    __syncthreads();  // buf[2], s_wagg[slot ^ 1] and the halo are reused next iteration
-  }
-
-  if (leader) {
-    for (int b = 0; b < 3; ++b)
-      if (inflight & (1u << b)) (void)mbar_wait(&s_bar[b], parity[b], spin_limit_ns);
+    p_tile = q_tile;
+    q_tile = t;
+    if (t == NONE && p_tile == NONE && q_tile == NONE) break;
   }
 }
 
@@ -448,7 +527,7 @@ int rbk_launch(const K *keys, const V *vals, uint64_t n, K *out_keys, V *out_val
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
   const int tma_ok = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals)) & 15) == 0;
-  const size_t smem = 3 * C::BUF_BYTES;
+  const size_t smem = (size_t)kRbkBufs * C::BUF_BYTES;
   static thread_local bool attr_set = false;
   if (!attr_set) {
     if ((st = host::set_smem_attrs(rbk_kernel<K, V>, smem)) != BK_OK) return st;
