@@ -176,47 +176,70 @@ struct LaneRun {
   int nvalid;     // elements of this lane inside the tile
 };
 
-// Element index of the lane's first element: e0 = (warp * 32 + lane) * M.
-// Neighbouring keys come from the adjacent lanes by shuffles; lane 0 / lane
-// 31 read the key before / after the warp's range from shared memory, or the
-// halo at the tile's edges (hb[0][KC-1] precedes the tile, hb[1][0] follows
-// it).  first_tile: the tile starts the input; last_tile: it ends it.
+// Loads a lane's M consecutive keys and values of a staged tile (element
+// index of its first: e0 = (warp * 32 + lane) * M); elements past the tile's
+// end read as key K() and value 0.
 template <typename K, typename V>
-__device__ __forceinline__ void rbk_read_lane(const unsigned char *buf, const K (*hb)[16 / sizeof(K)], uint32_t count,
-                                              bool first_tile, bool last_tile, int warp, int lane,
+__device__ __forceinline__ void rbk_load_lane(const unsigned char *buf, uint32_t count, int warp, int lane,
                                               LaneRun<K, V, RbkCfg<K, V>::M> &lr) {
   using C = RbkCfg<K, V>;
   constexpr int M = C::M;
-  constexpr int KC = 16 / sizeof(K);
-  const K *sk = reinterpret_cast<const K *>(buf);
   const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
   load_lane_rotated<M * sizeof(K)>(lr.key, buf, e0 * (uint32_t)sizeof(K), lane);
   load_lane_rotated<M * sizeof(V)>(lr.val, buf + C::KEY_BYTES, e0 * (uint32_t)sizeof(V), lane);
   const int nvalid = (int)min(max((int)count - (int)e0, 0), M);
   lr.nvalid = nvalid;
+  if (nvalid < M) {
 #pragma unroll
-  for (int j = 0; j < M; ++j)
-    if (j >= nvalid) {
-      lr.key[j] = K();
-      lr.val[j] = V(0);
-    }
+    for (int j = 0; j < M; ++j)
+      if (j >= nvalid) {
+        lr.key[j] = K();
+        lr.val[j] = V(0);
+      }
+  }
+}
+
+// Head and tail flags of a lane's loaded elements.  A head's key differs
+// from its predecessor's, so an element before a head is a tail; the lane's
+// last element compares with the next lane's first key, read by a shuffle
+// (lane 31: from shared memory, or the halo hb[1][0] after the tile).  Lane 0
+// reads the key before the warp's range from shared memory, or the halo
+// hb[0][KC-1] before the tile.  first_tile: the tile starts the input;
+// last_tile: it ends it.
+template <typename K, typename V>
+__device__ __forceinline__ void rbk_flags(const unsigned char *buf, const K (*hb)[16 / sizeof(K)], uint32_t count,
+                                          bool first_tile, bool last_tile, int warp, int lane,
+                                          LaneRun<K, V, RbkCfg<K, V>::M> &lr) {
+  using C = RbkCfg<K, V>;
+  constexpr int M = C::M;
+  constexpr int KC = 16 / sizeof(K);
+  const K *sk = reinterpret_cast<const K *>(buf);
+  const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
+  const int nvalid = lr.nvalid;
   K prev = shfl_up(lr.key[M - 1], 1);
   K next = shfl_down_any(lr.key[0], 1);
   if (lane == 0) prev = e0 == 0 ? hb[0][KC - 1] : sk[e0 - 1];
   if (lane == 31) next = e0 + M < count ? sk[e0 + M] : hb[1][0];
-  uint32_t head = 0, tail = 0;
+  uint32_t head = 0;
 #pragma unroll
   for (int j = 0; j < M; ++j) {
     const K pk = j == 0 ? prev : lr.key[j - 1];
-    const bool h = (j < nvalid) && !(lr.key[j] == pk);
-    head |= (uint32_t)h << j;
-    // successor inside the lane, in the next lane / warp, or after the tile
-    const bool last_of_tile = (e0 + j + 1 == count);
-    const K nk = j + 1 < M ? lr.key[j + 1] : next;
-    const bool t = (j < nvalid) && (last_of_tile ? (last_tile || !(hb[1][0] == lr.key[j])) : !(nk == lr.key[j]));
-    tail |= (uint32_t)t << j;
+    head |= (uint32_t)((j < nvalid) && !(lr.key[j] == pk)) << j;
   }
   if (first_tile && e0 == 0 && nvalid > 0) head |= 1u;  // the input's first element
+  // element j < nvalid - 1 ends a run exactly when j + 1 starts one
+  uint32_t tail = nvalid > 0 ? (head >> 1) & ((1u << (nvalid - 1)) - 1u) : 0u;
+  if (nvalid == M) {
+    const bool tile_end = e0 + M == count;
+    const bool tl = tile_end ? (last_tile || !(hb[1][0] == lr.key[M - 1])) : !(next == lr.key[M - 1]);
+    tail |= (uint32_t)tl << (M - 1);
+  } else if (nvalid > 0) {  // the lane holding the tile's last element
+    K kl = lr.key[0];
+#pragma unroll
+    for (int j = 1; j < M; ++j)
+      if (j == nvalid - 1) kl = lr.key[j];
+    tail |= (uint32_t)(last_tile || !(hb[1][0] == kl)) << (nvalid - 1);
+  }
   lr.head = head;
   lr.tail = tail;
 }
@@ -261,6 +284,12 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
   __shared__ __align__(8) uint64_t s_qbar[Q];
   __shared__ unsigned int s_ticket[NB];
   __shared__ P s_wagg[4][kRbkWarps];  // per-warp (c, v) of t_i, by iteration mod 4
+  // phase 1's per-lane results, kept for phase 2 (each warp reads back only
+  // its own lanes, so program order protects them; by iteration mod 3):
+  // head flags | tail flags << 16, and the lane's exclusive (c, v) in its warp
+  __shared__ uint32_t s_lflags[3][32 * kRbkWarps];
+  __shared__ uint32_t s_lc[3][32 * kRbkWarps];
+  __shared__ V s_lv[3][32 * kRbkWarps];
   __shared__ unsigned int s_q_tile[Q];
   __shared__ P s_q_agg[Q];
   __shared__ P s_q_prefix[Q];
@@ -429,9 +458,16 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
     if (t != NONE) {
       const uint32_t count = tile_count(t);
       LaneRun<K, V, M> lr;
-      rbk_read_lane<K, V>(buf(bt), s_halo[bt], count, t == 0, (uint64_t)t * TILE + count == n, warp, lane, lr);
+      rbk_load_lane<K, V>(buf(bt), count, warp, lane, lr);
+      rbk_flags<K, V>(buf(bt), s_halo[bt], count, t == 0, (uint64_t)t * TILE + count == n, warp, lane, lr);
       const P incl = warp_inclusive_scan(lane_fold(lr), op, lane);
       if (lane == 31) s_wagg[it & 3][warp] = incl;
+      P lex = shfl_up(incl, 1);
+      if (lane == 0) lex = OpSeg<V>::identity();
+      const int sl = it % 3, li = warp * 32 + lane;
+      s_lflags[sl][li] = lr.head | (lr.tail << 16);
+      s_lc[sl][li] = lex.c;
+      s_lv[sl][li] = lex.v;
     }
     __syncwarp();
     if (!bad && lane == 0) mbar_arrive(&s_p1[bt]);
@@ -463,32 +499,29 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
       const uint32_t count = tile_count(p);
       const bool last_tile = (uint64_t)p * TILE + count == n;
       LaneRun<K, V, M> lr;
-      rbk_read_lane<K, V>(buf(bp), s_halo[bp], count, p == 0, last_tile, warp, lane, lr);
-      const P lane_incl = warp_inclusive_scan(lane_fold(lr), op, lane);
+      rbk_load_lane<K, V>(buf(bp), count, warp, lane, lr);
+      const int sl = (it + 1) % 3, li = warp * 32 + lane;  // phase 1 of p ran at it - 2
+      const uint32_t fl = s_lflags[sl][li];
+      const uint32_t head = fl & 0xffffu, tail = fl >> 16;
       P carry = s_q_prefix[e % Q];
       for (int i = 0; i < warp; ++i) carry = op(carry, s_wagg[(it + 2) & 3][i]);
-      const P excl = shfl_up(lane_incl, 1);
-      if (lane > 0) carry = op(carry, excl);
-      // walk the lane's elements with the running (c, v); each tail emits its run
-      const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
+      carry = op(carry, P{s_lc[sl][li], s_lv[sl][li]});
+      // walk the lane's elements with the running (c, v); each tail emits its
+      // run (elements past the tile's end have no flags and value 0)
       uint32_t c = carry.c;
       V v = carry.v;
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        if (j < lr.nvalid) {
-          if (lr.head & (1u << j)) {
-            ++c;
-            v = lr.val[j];
-          } else {
-            v = (V)(v + lr.val[j]);
-          }
-          if (lr.tail & (1u << j)) {
-            out_keys[c - 1] = lr.key[j];
-            out_vals[c - 1] = v;
-            if (last_tile && e0 + j + 1 == count) *d_num_out = c;
-          }
+        const bool h = (head >> j) & 1u;
+        c += h ? 1u : 0u;
+        v = h ? lr.val[j] : (V)(v + lr.val[j]);
+        if ((tail >> j) & 1u) {
+          out_keys[c - 1] = lr.key[j];
+          out_vals[c - 1] = v;
         }
       }
+      const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
+      if (last_tile && e0 < count && count <= e0 + M) *d_num_out = c;  // this lane holds the input's last element
     }
     __syncwarp();
     if (!bad && lane == 0) mbar_arrive(&s_p2[bp]);
