@@ -18,4 +18,6 @@ from .algorithms import (  # noqa: F401
     workspaces,
 )
 
+from .batch import BATCH_MAX, batch_workspace_bytes, inclusive_scan_batch, reduce_by_key_batch  # noqa: F401
+
 __version__ = "1.0.0"

@@ -81,6 +81,70 @@ __global__ void rbk_init_kernel(Status st, size_t tiles, WsHeader *hdr) {
 template <typename V>
 __global__ void write_count_kernel(uint64_t *d_num_out) { *d_num_out = 0; }
 
+// Where one tile lives: its array (keys, values, length, outputs) and its
+// index within that array.
+template <typename K, typename V>
+struct RbkTile {
+  const K *keys;
+  const V *vals;
+  uint64_t n;
+  uint32_t local;  // tile index within the array
+  K *out_keys;
+  V *out_vals;
+  uint64_t *num_out;
+  bool tma;        // keys and vals 16-byte aligned
+  __device__ __forceinline__ uint32_t count() const {
+    const uint64_t base = (uint64_t)local * RbkCfg<K, V>::TILE;
+    return (uint32_t)((n - base) < (uint64_t)RbkCfg<K, V>::TILE ? (n - base) : (uint64_t)RbkCfg<K, V>::TILE);
+  }
+  __device__ __forceinline__ bool first() const { return local == 0u; }
+  __device__ __forceinline__ bool last() const { return (uint64_t)local * RbkCfg<K, V>::TILE + count() == n; }
+};
+
+// Tile source: one array.
+template <typename K, typename V>
+struct RbkOne {
+  const K *keys;
+  const V *vals;
+  uint64_t n;
+  K *out_keys;
+  V *out_vals;
+  uint64_t *num_out;
+  int tma;
+  int any_unaligned;
+  __device__ __forceinline__ RbkTile<K, V> tile(unsigned int t) const {
+    return RbkTile<K, V>{keys, vals, n, t, out_keys, out_vals, num_out, tma != 0};
+  }
+};
+
+// Tile source: a batch of independent arrays reduced by one launch.  Array i
+// owns global tiles [start[i], start[i + 1]); its first tile publishes an
+// inclusive prefix at once, so no look-back crosses into another array.  The
+// descriptors travel in the kernel's parameters.
+constexpr int kRbkBatchMax = 256;
+template <typename K, typename V>
+struct RbkBatch {
+  const K *keys[kRbkBatchMax];
+  const V *vals[kRbkBatchMax];
+  uint64_t n[kRbkBatchMax];
+  K *out_keys[kRbkBatchMax];
+  V *out_vals[kRbkBatchMax];
+  uint64_t *num_out[kRbkBatchMax];
+  uint32_t start[kRbkBatchMax + 1];
+  uint32_t count;
+  int any_unaligned;
+  __device__ __forceinline__ RbkTile<K, V> tile(unsigned int t) const {
+    int lo = 0, hi = (int)count - 1;  // the last array whose first tile is <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (start[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const bool tma = ((reinterpret_cast<uintptr_t>(keys[lo]) | reinterpret_cast<uintptr_t>(vals[lo])) & 15) == 0;
+    return RbkTile<K, V>{keys[lo], vals[lo], n[lo], t - start[lo], out_keys[lo], out_vals[lo], num_out[lo], tma};
+  }
+};
+
 // Leader: load tile `tile` (keys, values and the halo keys on either side)
 // into buffer `buf`.  The halo keys arrive as the aligned 16-byte chunks that
 // hold them (hb[0]: the chunk ending just before the tile, hb[1]: the chunk
@@ -264,13 +328,11 @@ __device__ __forceinline__ Seg<V> lane_fold(const LaneRun<K, V, M> &lr) {
 // a buffer once the compute warps are done reading it, with no store to
 // drain; and without TMA (pointers not 16-byte aligned) the compute warps
 // stage both tiles themselves between two compute-only barriers.
-template <typename K, typename V>
-__global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, const V *vals, uint64_t n, K *out_keys,
-                                                             V *out_vals, uint64_t *d_num_out,
+template <typename K, typename V, typename Src>
+__global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_constant__ Src src,
                                                              typename RbkCfg<K, V>::Status st, WsHeader *hdr,
                                                              unsigned long long spin_limit_ns,
-                                                             long long skip_publish_tile, int tma_ok,
-                                                             unsigned int num_tiles) {
+                                                             long long skip_publish_tile, unsigned int num_tiles) {
   using C = RbkCfg<K, V>;
   using P = typename C::P;
   constexpr int M = C::M, TILE = C::TILE, NB = kRbkBufs, Q = kRbkQueue;
@@ -299,10 +361,6 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
   auto abort_now = [&]() { *reinterpret_cast<volatile int *>(&s_abort) = 1; };
   auto aborted = [&]() -> bool { return *reinterpret_cast<volatile int *>(&s_abort) != 0; };
   auto buf = [&](int b) { return smem_raw + (size_t)b * C::BUF_BYTES; };
-  auto tile_count = [&](unsigned int tile) -> uint32_t {
-    const uint64_t base = (uint64_t)tile * TILE;
-    return (uint32_t)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
-  };
 
   uint64_t keep = 0, stream = 0;
   uint32_t armed[NB];  // loader: phases armed on s_full[b]
@@ -326,7 +384,10 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
     t_first = t0 < num_tiles ? t0 : NONE;
     s_ticket[0] = t_first;
     bool tx = false;
-    if (t_first != NONE) tx = rbk_issue_load<K, V>(keys, vals, n, t_first, buf(0), s_halo[0], &s_full[0], keep, tma_ok);
+    if (t_first != NONE) {
+      const RbkTile<K, V> tl = src.tile(t_first);
+      tx = rbk_issue_load<K, V>(tl.keys, tl.vals, tl.n, tl.local, buf(0), s_halo[0], &s_full[0], keep, tl.tma);
+    }
     if (!tx) mbar_arrive(&s_full[0]);
     armed[0] = 1u;
     mbar_arrive(&s_full[NB - 1]);  // iteration 0's phase 2 reads buffer NB - 1: an empty phase
@@ -348,7 +409,10 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
       const unsigned int tn = (t != NONE && next_raw < num_tiles) ? next_raw : NONE;
       s_ticket[bn] = tn;
       bool tx = false;
-      if (tn != NONE) tx = rbk_issue_load<K, V>(keys, vals, n, tn, buf(bn), s_halo[bn], &s_full[bn], keep, tma_ok);
+      if (tn != NONE) {
+        const RbkTile<K, V> tl = src.tile(tn);
+        tx = rbk_issue_load<K, V>(tl.keys, tl.vals, tl.n, tl.local, buf(bn), s_halo[bn], &s_full[bn], keep, tl.tma);
+      }
       if (!tx) mbar_arrive(&s_full[bn]);
       ++armed[bn];
       next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
@@ -360,8 +424,10 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
       }
       p1par[bt] ^= 1u;
       tx = false;
-      if (q_tile != NONE)
-        tx = rbk_issue_load<K, V>(keys, vals, n, q_tile, buf(bt), s_halo[bt], &s_full[bt], stream, tma_ok);
+      if (q_tile != NONE) {
+        const RbkTile<K, V> tl = src.tile(q_tile);
+        tx = rbk_issue_load<K, V>(tl.keys, tl.vals, tl.n, tl.local, buf(bt), s_halo[bt], &s_full[bt], stream, tl.tma);
+      }
       if (!tx) mbar_arrive(&s_full[bt]);
       ++armed[bt];
       // buffer bp is free once phase 2 of p has read it
@@ -414,12 +480,13 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
       if (q == NONE) break;
       if (!wait_queued(j + 2u)) break;
       const P agg = s_q_agg[j % Q];
+      const bool qfirst = src.tile(q).first();
       P excl = OpSeg<V>::identity();
       bool ok = true;
-      if (q != 0) ok = lookback_exclusive<P>(st, q, op, excl, hdr, spin_limit_ns);
+      if (!qfirst) ok = lookback_exclusive<P>(st, q, op, excl, hdr, spin_limit_ns);
       if (lane == 0) {
         if (ok) {
-          if (q != 0 && (long long)q != skip_publish_tile) st.publish(q, kStPrefix, op(excl, agg));
+          if (!qfirst && (long long)q != skip_publish_tile) st.publish(q, kStPrefix, op(excl, agg));
           s_q_prefix[j % Q] = excl;
           mbar_arrive(&s_qbar[j % Q]);
         } else {
@@ -448,18 +515,26 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
     fpar[bt] ^= 1u;
     bad = __any_sync(0xffffffffu, bad);
     if (!bad) t = s_ticket[bt];
-    if (!tma_ok) {
-      // stage t and p here (previous iteration's readers are past the first barrier)
+    if (src.any_unaligned) {
+      // stage the tiles that have no TMA copy here (previous iteration's
+      // readers are past the first barrier)
       named_barrier_sync(2, 32 * kRbkWarps);
-      if (t != NONE) rbk_sync_load<K, V>(keys, vals, n, t, buf(bt));
-      if (p != NONE) rbk_sync_load<K, V>(keys, vals, n, p, buf(bp));
+      if (t != NONE) {
+        const RbkTile<K, V> tl = src.tile(t);
+        if (!tl.tma) rbk_sync_load<K, V>(tl.keys, tl.vals, tl.n, tl.local, buf(bt));
+      }
+      if (p != NONE) {
+        const RbkTile<K, V> tl = src.tile(p);
+        if (!tl.tma) rbk_sync_load<K, V>(tl.keys, tl.vals, tl.n, tl.local, buf(bp));
+      }
       named_barrier_sync(2, 32 * kRbkWarps);
     }
     if (t != NONE) {
-      const uint32_t count = tile_count(t);
+      const RbkTile<K, V> tl = src.tile(t);
+      const uint32_t count = tl.count();
       LaneRun<K, V, M> lr;
       rbk_load_lane<K, V>(buf(bt), count, warp, lane, lr);
-      rbk_flags<K, V>(buf(bt), s_halo[bt], count, t == 0, (uint64_t)t * TILE + count == n, warp, lane, lr);
+      rbk_flags<K, V>(buf(bt), s_halo[bt], count, tl.first(), tl.last(), warp, lane, lr);
       const P incl = warp_inclusive_scan(lane_fold(lr), op, lane);
       if (lane == 31) s_wagg[it & 3][warp] = incl;
       P lex = shfl_up(incl, 1);
@@ -479,7 +554,7 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
       if (t != NONE) {
 #pragma unroll
         for (int i = 0; i < kRbkWarps; ++i) agg = op(agg, s_wagg[it & 3][i]);
-        if ((long long)t != skip_publish_tile) st.publish(t, t == 0 ? kStPrefix : kStAggregate, agg);
+        if ((long long)t != skip_publish_tile) st.publish(t, src.tile(t).first() ? kStPrefix : kStAggregate, agg);
       }
       s_q_tile[it % Q] = t;
       s_q_agg[it % Q] = agg;
@@ -496,8 +571,9 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
     bad = __any_sync(0xffffffffu, bad);
     if (p != NONE && !bad) {
       const unsigned int e = (unsigned int)it - 2u;
-      const uint32_t count = tile_count(p);
-      const bool last_tile = (uint64_t)p * TILE + count == n;
+      const RbkTile<K, V> tl = src.tile(p);
+      const uint32_t count = tl.count();
+      const bool last_tile = tl.last();
       LaneRun<K, V, M> lr;
       rbk_load_lane<K, V>(buf(bp), count, warp, lane, lr);
       const int sl = (it + 1) % 3, li = warp * 32 + lane;  // phase 1 of p ran at it - 2
@@ -516,12 +592,12 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
         c += h ? 1u : 0u;
         v = h ? lr.val[j] : (V)(v + lr.val[j]);
         if ((tail >> j) & 1u) {
-          out_keys[c - 1] = lr.key[j];
-          out_vals[c - 1] = v;
+          tl.out_keys[c - 1] = lr.key[j];
+          tl.out_vals[c - 1] = v;
         }
       }
       const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
-      if (last_tile && e0 < count && count <= e0 + M) *d_num_out = c;  // this lane holds the input's last element
+      if (last_tile && e0 < count && count <= e0 + M) *tl.num_out = c;  // this lane holds the input's last element
     }
     __syncwarp();
     if (!bad && lane == 0) mbar_arrive(&s_p2[bp]);
@@ -532,25 +608,16 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const K *keys, cons
   }
 }
 
-template <typename K, typename V>
-int rbk_launch(const K *keys, const V *vals, uint64_t n, K *out_keys, V *out_vals, uint64_t *d_num_out, void *d_ws,
-               size_t ws_bytes, cudaStream_t stream) {
+// Clears the status words, then runs the persistent reduce_by_key over
+// `tiles` tiles of `src` (one array or a batch).
+template <typename K, typename V, typename Src>
+int rbk_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
   using C = RbkCfg<K, V>;
   host::DeviceInfo di;
   int st = host::device_info(&di);
   if (st != BK_OK) return st;
-  if (d_num_out == nullptr) return BK_ERR_INVALID_ARGUMENT;
-  if (n == 0) {
-    write_count_kernel<V><<<1, 1, 0, stream>>>(d_num_out);
-    return host::launch_status();
-  }
-  if (keys == nullptr || vals == nullptr || out_keys == nullptr || out_vals == nullptr) return BK_ERR_INVALID_ARGUMENT;
-  if (!host::aligned_to<K>(keys) || !host::aligned_to<V>(vals) || !host::aligned_to<K>(out_keys) ||
-      !host::aligned_to<V>(out_vals) || !host::aligned_to<uint64_t>(d_num_out))
-    return BK_ERR_MISALIGNED;
-  if (n >= 0xffffffffull) return BK_ERR_TOO_LARGE;  // run counts are 32-bit
-  const size_t tiles = rbk_num_tiles<K, V>(n);
-  st = host::check_ws(d_ws, ws_bytes, rbk_ws_bytes<K, V>(n));
+  if (tiles >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
+  st = host::check_ws(d_ws, ws_bytes, kHeaderBytes + C::Status::bytes(tiles));
   if (st != BK_OK) return st;
   WsHeader *hdr = reinterpret_cast<WsHeader *>(d_ws);
   auto status = C::Status::at(reinterpret_cast<char *>(d_ws) + kHeaderBytes, tiles);
@@ -559,17 +626,111 @@ int rbk_launch(const K *keys, const V *vals, uint64_t n, K *out_keys, V *out_val
   if ((st = host::launch_status()) != BK_OK) return st;
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
-  const int tma_ok = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals)) & 15) == 0;
   const size_t smem = (size_t)kRbkBufs * C::BUF_BYTES;
   static thread_local bool attr_set = false;
   if (!attr_set) {
-    if ((st = host::set_smem_attrs(rbk_kernel<K, V>, smem)) != BK_OK) return st;
+    if ((st = host::set_smem_attrs(rbk_kernel<K, V, Src>, smem)) != BK_OK) return st;
     attr_set = true;
   }
   const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * 2);
-  rbk_kernel<K, V><<<grid, kRbkThreads, smem, stream>>>(keys, vals, n, out_keys, out_vals, d_num_out, status, hdr,
-                                                        limit, dbg.skip_publish_tile, tma_ok, (unsigned)tiles);
+  rbk_kernel<K, V, Src><<<grid, kRbkThreads, smem, stream>>>(src, status, hdr, limit, dbg.skip_publish_tile,
+                                                            (unsigned)tiles);
   return host::launch_status();
+}
+
+template <typename K, typename V>
+int rbk_check_array(const K *keys, const V *vals, uint64_t n, K *out_keys, V *out_vals, uint64_t *d_num_out) {
+  if (d_num_out == nullptr) return BK_ERR_INVALID_ARGUMENT;
+  if (n > 0 && (keys == nullptr || vals == nullptr || out_keys == nullptr || out_vals == nullptr))
+    return BK_ERR_INVALID_ARGUMENT;
+  if (!host::aligned_to<K>(keys) || !host::aligned_to<V>(vals) || !host::aligned_to<K>(out_keys) ||
+      !host::aligned_to<V>(out_vals) || !host::aligned_to<uint64_t>(d_num_out))
+    return BK_ERR_MISALIGNED;
+  if (n >= 0xffffffffull) return BK_ERR_TOO_LARGE;  // run counts are 32-bit
+  return BK_OK;
+}
+
+template <typename K, typename V>
+int rbk_launch(const K *keys, const V *vals, uint64_t n, K *out_keys, V *out_vals, uint64_t *d_num_out, void *d_ws,
+               size_t ws_bytes, cudaStream_t stream) {
+  host::DeviceInfo di;
+  int st = host::device_info(&di);
+  if (st != BK_OK) return st;
+  if ((st = rbk_check_array(keys, vals, n, out_keys, out_vals, d_num_out)) != BK_OK) return st;
+  if (n == 0) {
+    write_count_kernel<V><<<1, 1, 0, stream>>>(d_num_out);
+    return host::launch_status();
+  }
+  const int tma = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals)) & 15) == 0;
+  const RbkOne<K, V> src{keys, vals, n, out_keys, out_vals, d_num_out, tma, !tma};
+  return rbk_run<K, V>(src, rbk_num_tiles<K, V>(n), d_ws, ws_bytes, stream);
+}
+
+// A batch item as the C-ABI passes it (bk_rbk_item_<key>_<value>).
+template <typename K, typename V>
+struct RbkItem {
+  const K *keys;
+  const V *vals;
+  uint64_t n;
+  K *out_keys;
+  V *out_vals;
+  uint64_t *d_num_out;
+};
+
+template <typename K, typename V>
+int rbk_batch_launch(const RbkItem<K, V> *items, uint32_t count, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
+  host::DeviceInfo di;
+  int st = host::device_info(&di);
+  if (st != BK_OK) return st;
+  if (count > 0 && items == nullptr) return BK_ERR_INVALID_ARGUMENT;
+  if (count > (uint32_t)kRbkBatchMax) return BK_ERR_TOO_LARGE;
+  RbkBatch<K, V> b;
+  b.count = 0;
+  b.any_unaligned = 0;
+  size_t tiles = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const RbkItem<K, V> &it = items[i];
+    if ((st = rbk_check_array(it.keys, it.vals, it.n, it.out_keys, it.out_vals, it.d_num_out)) != BK_OK) return st;
+    if (it.n == 0) {  // no tile: its count is written here
+      write_count_kernel<V><<<1, 1, 0, stream>>>(it.d_num_out);
+      if ((st = host::launch_status()) != BK_OK) return st;
+      continue;
+    }
+    const uint32_t k = b.count++;
+    b.keys[k] = it.keys;
+    b.vals[k] = it.vals;
+    b.n[k] = it.n;
+    b.out_keys[k] = it.out_keys;
+    b.out_vals[k] = it.out_vals;
+    b.num_out[k] = it.d_num_out;
+    b.start[k] = (uint32_t)tiles;
+    if (((reinterpret_cast<uintptr_t>(it.keys) | reinterpret_cast<uintptr_t>(it.vals)) & 15) != 0) b.any_unaligned = 1;
+    tiles += rbk_num_tiles<K, V>(it.n);
+    if (tiles >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
+  }
+  b.start[b.count] = (uint32_t)tiles;
+  if (b.count == 0) return BK_OK;
+  return rbk_run<K, V>(b, tiles, d_ws, ws_bytes, stream);
+}
+
+template <typename K, typename V>
+size_t rbk_batch_ws(const uint64_t *sizes, uint32_t count) {
+  size_t tiles = 0;
+  for (uint32_t i = 0; i < count; ++i) tiles += rbk_num_tiles<K, V>(sizes[i]);
+  return kHeaderBytes + RbkCfg<K, V>::Status::bytes(tiles);
+}
+
+size_t rbk_batch_workspace_bytes(int key_dtype, int value_dtype, const uint64_t *sizes, uint32_t count) {
+  if (count > 0 && sizes == nullptr) return 0;
+  const bool k4 = key_dtype == BK_DTYPE_I32 || key_dtype == BK_DTYPE_U32;
+  const bool k8 = key_dtype == BK_DTYPE_I64 || key_dtype == BK_DTYPE_U64;
+  const bool v4 = value_dtype == BK_DTYPE_I32 || value_dtype == BK_DTYPE_U32 || value_dtype == BK_DTYPE_F32;
+  const bool v8 = value_dtype == BK_DTYPE_I64 || value_dtype == BK_DTYPE_U64 || value_dtype == BK_DTYPE_F64;
+  if (k4 && v4) return rbk_batch_ws<int32_t, float>(sizes, count);
+  if (k4 && v8) return rbk_batch_ws<int32_t, double>(sizes, count);
+  if (k8 && v4) return rbk_batch_ws<int64_t, float>(sizes, count);
+  if (k8 && v8) return rbk_batch_ws<int64_t, double>(sizes, count);
+  return 0;
 }
 
 size_t rbk_workspace_bytes(int key_dtype, int value_dtype, uint64_t n) {
@@ -604,3 +765,22 @@ BK_DEFINE_RBK(i64, int64_t, i32, int32_t)
 BK_DEFINE_RBK(i64, int64_t, i64, int64_t)
 BK_DEFINE_RBK(i64, int64_t, f32, float)
 BK_DEFINE_RBK(i64, int64_t, f64, double)
+
+#define BK_DEFINE_RBK_BATCH(KN, K, VN, V)                                                                      \
+  static_assert(sizeof(bk_rbk_item_##KN##_##VN) == sizeof(bk::RbkItem<K, V>), "bk_rbk_item layout");        \
+  extern "C" int bk_reduce_by_key_##KN##_##VN##_batch(const bk_rbk_item_##KN##_##VN *items, uint32_t count,  \
+                                                      void *d_ws, size_t ws_bytes, bk_stream_t stream) {     \
+    return bk::rbk_batch_launch<K, V>(reinterpret_cast<const bk::RbkItem<K, V> *>(items), count, d_ws,        \
+                                      ws_bytes, (cudaStream_t)stream);                                        \
+  }
+
+BK_DEFINE_RBK_BATCH(i32, int32_t, i32, int32_t)
+BK_DEFINE_RBK_BATCH(i32, int32_t, i64, int64_t)
+BK_DEFINE_RBK_BATCH(i32, int32_t, f32, float)
+BK_DEFINE_RBK_BATCH(i32, int32_t, f64, double)
+BK_DEFINE_RBK_BATCH(u32, uint32_t, f32, float)
+BK_DEFINE_RBK_BATCH(u32, uint32_t, f64, double)
+BK_DEFINE_RBK_BATCH(i64, int64_t, i32, int32_t)
+BK_DEFINE_RBK_BATCH(i64, int64_t, i64, int64_t)
+BK_DEFINE_RBK_BATCH(i64, int64_t, f32, float)
+BK_DEFINE_RBK_BATCH(i64, int64_t, f64, double)

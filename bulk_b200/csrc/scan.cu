@@ -63,38 +63,77 @@ __global__ void lookback_init_kernel(Status st, size_t tiles, WsHeader *hdr) {
   if (i == 0) hdr->tile_ticket = 0u;
 }
 
-// Copies tile `tile` of `src` into shared memory `buf`: the 16-byte-aligned
-// body with one TMA bulk copy completing on `bar` (returns whether one was
-// issued), the ragged tail (fewer than V elements) with plain loads by the
-// calling thread.  Called by one thread.
+// Where one tile lives.
 template <typename T>
-__device__ __forceinline__ bool scan_issue_tile_load(const T *src, uint64_t n, unsigned int tile, T *buf,
-                                                     uint64_t *bar, uint64_t policy) {
+struct ScanTile {
+  const T *in;     // the tile's first input element
+  T *out;          // its first output element
+  uint32_t count;  // elements in the tile
+  bool first;      // first tile of its array: publishes its inclusive prefix at once
+  bool tma;        // in and out 16-byte aligned
+  T init;          // its array's init
+};
+
+// Tile source: one array.
+template <typename T>
+struct ScanOne {
+  const T *in;
+  T *out;
+  uint64_t n;
+  T init;
+  int tma;
+  __device__ __forceinline__ ScanTile<T> tile(unsigned int t) const {
+    const uint64_t base = (uint64_t)t * ScanCfg<T>::TILE;
+    const uint64_t rem = n - base;
+    return ScanTile<T>{in + base, out + base,
+                       (uint32_t)(rem < (uint64_t)ScanCfg<T>::TILE ? rem : (uint64_t)ScanCfg<T>::TILE), t == 0u,
+                       tma != 0, init};
+  }
+};
+
+// Tile source: a batch of independent arrays scanned by one launch.  Array
+// i owns global tiles [start[i], start[i + 1]); its first tile publishes an
+// inclusive prefix at once, so no look-back crosses into another array.  The
+// descriptors travel in the kernel's parameters.
+constexpr int kScanBatchMax = 256;
+template <typename T>
+struct ScanBatch {
+  const T *in[kScanBatchMax];
+  T *out[kScanBatchMax];
+  uint64_t n[kScanBatchMax];
+  T init[kScanBatchMax];
+  uint32_t start[kScanBatchMax + 1];
+  uint32_t count;
+  __device__ __forceinline__ ScanTile<T> tile(unsigned int t) const {
+    int lo = 0, hi = (int)count - 1;  // the last array whose first tile is <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (start[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint32_t local = t - start[lo];
+    const uint64_t base = (uint64_t)local * ScanCfg<T>::TILE;
+    const uint64_t rem = n[lo] - base;
+    const bool tma = ((reinterpret_cast<uintptr_t>(in[lo]) | reinterpret_cast<uintptr_t>(out[lo])) & 15) == 0;
+    return ScanTile<T>{in[lo] + base, out[lo] + base,
+                       (uint32_t)(rem < (uint64_t)ScanCfg<T>::TILE ? rem : (uint64_t)ScanCfg<T>::TILE),
+                       local == 0u, tma, init[lo]};
+  }
+};
+
+// Copies a tile into shared memory `buf`: the 16-byte-aligned body with one
+// TMA bulk copy completing on `bar` (returns whether one was issued), the
+// ragged tail (fewer than V elements) with plain loads by the calling thread.
+// Called by one thread, only for tiles whose pointers are 16-byte aligned.
+template <typename T>
+__device__ __forceinline__ bool scan_issue_tile_load(const ScanTile<T> &tl, T *buf, uint64_t *bar, uint64_t policy) {
   using C = ScanCfg<T>;
-  const uint64_t base = (uint64_t)tile * C::TILE;
-  const uint32_t count = (uint32_t)((n - base) < (uint64_t)C::TILE ? (n - base) : (uint64_t)C::TILE);
-  const uint32_t bulk = count & ~(uint32_t)(C::V - 1);
-  for (uint32_t i = bulk; i < count; ++i) buf[i] = src[base + i];
+  const uint32_t bulk = tl.count & ~(uint32_t)(C::V - 1);
+  for (uint32_t i = bulk; i < tl.count; ++i) buf[i] = tl.in[i];
   if (bulk == 0) return false;
   mbar_arrive_expect_tx(bar, bulk * (uint32_t)sizeof(T));
-  tma_load_1d_hint(buf, src + base, bulk * (uint32_t)sizeof(T), bar, policy);
+  tma_load_1d_hint(buf, tl.in, bulk * (uint32_t)sizeof(T), bar, policy);
   return true;
-}
-
-// All threads: plain coalesced copy of a tile into shared memory (used when
-// the pointers are not 16-byte aligned).
-template <typename T>
-__device__ __forceinline__ void scan_sync_tile_load(const T *src, uint64_t n, unsigned int tile, T *buf) {
-  using C = ScanCfg<T>;
-  const uint64_t base = (uint64_t)tile * C::TILE;
-  const uint32_t count = (uint32_t)((n - base) < (uint64_t)C::TILE ? (n - base) : (uint64_t)C::TILE);
-  for (uint32_t i = threadIdx.x; i < count; i += kScanWarps * 32) buf[i] = src[base + i];
-}
-
-template <typename T>
-__device__ __forceinline__ uint32_t scan_tile_count(uint64_t n, unsigned int tile) {
-  const uint64_t base = (uint64_t)tile * ScanCfg<T>::TILE;
-  return (uint32_t)((n - base) < (uint64_t)ScanCfg<T>::TILE ? (n - base) : (uint64_t)ScanCfg<T>::TILE);
 }
 
 // Persistent two-phase scan.  Warps 0-7 compute, warp 8 (lane 0) loads and
@@ -133,12 +172,11 @@ __device__ __forceinline__ uint32_t scan_tile_count(uint64_t n, unsigned int til
 // depends only on its load and on a look-back for a still lower tile, so the
 // waits always end; every wait is still bounded by spin_limit_ns and gives up
 // at once when anyone in the CTA has failed.
-template <typename T, typename Op>
-__global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *out, uint64_t n, T init,
+template <typename T, typename Op, typename Src>
+__global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_constant__ Src src,
                                                                typename ScanCfg<T>::Status st, WsHeader *hdr,
                                                                unsigned long long spin_limit_ns,
-                                                               long long skip_publish_tile, int tma_ok,
-                                                               unsigned int num_tiles) {
+                                                               long long skip_publish_tile, unsigned int num_tiles) {
   using C = ScanCfg<T>;
   constexpr int V = C::V, TILE = C::TILE, R = kScanRowsPerWarp, NB = kScanBufs, Q = kScanQueue;
   constexpr unsigned int NONE = 0xffffffffu;
@@ -159,7 +197,9 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   // a TMA copy exists for `tile` exactly when this holds (scan_issue_tile_load)
   auto has_tma = [&](unsigned int tile) -> bool {
-    return tma_ok && tile != NONE && (scan_tile_count<T>(n, tile) & ~(uint32_t)(V - 1)) != 0u;
+    if (tile == NONE) return false;
+    const ScanTile<T> tl = src.tile(tile);
+    return tl.tma && (tl.count & ~(uint32_t)(V - 1)) != 0u;
   };
   auto abort_now = [&]() { *reinterpret_cast<volatile int *>(&s_abort) = 1; };
   auto aborted = [&]() -> bool { return *reinterpret_cast<volatile int *>(&s_abort) != 0; };
@@ -187,7 +227,10 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
     t_first = t0 < num_tiles ? t0 : NONE;
     s_ticket[0] = t_first;
     bool tx = false;
-    if (t_first != NONE && tma_ok) tx = scan_issue_tile_load(in, n, t_first, buf(0), &s_full[0], keep);
+    if (t_first != NONE) {
+      const ScanTile<T> tl = src.tile(t_first);
+      if (tl.tma) tx = scan_issue_tile_load(tl, buf(0), &s_full[0], keep);
+    }
     if (!tx) mbar_arrive(&s_full[0]);
     armed[0] = 1u;
     // iteration 0's phase 2 reads buffer NB - 1, which no re-read filled:
@@ -213,9 +256,12 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
       const unsigned int tn = (t != NONE && next_raw < num_tiles) ? next_raw : NONE;
       s_ticket[bn] = tn;
       bool tx = false;
-      if (tn != NONE && tma_ok) {
-        if (issued_store) tma_store_wait_read();
-        tx = scan_issue_tile_load(in, n, tn, buf(bn), &s_full[bn], keep);
+      if (tn != NONE) {
+        const ScanTile<T> tl = src.tile(tn);
+        if (tl.tma) {
+          if (issued_store) tma_store_wait_read();
+          tx = scan_issue_tile_load(tl, buf(bn), &s_full[bn], keep);
+        }
       }
       if (!tx) mbar_arrive(&s_full[bn]);
       ++armed[bn];
@@ -229,7 +275,10 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
       }
       p1par[bt] ^= 1u;
       tx = false;
-      if (q_tile != NONE && tma_ok) tx = scan_issue_tile_load(in, n, q_tile, buf(bt), &s_full[bt], stream);
+      if (q_tile != NONE) {
+        const ScanTile<T> tl = src.tile(q_tile);
+        if (tl.tma) tx = scan_issue_tile_load(tl, buf(bt), &s_full[bt], stream);
+      }
       if (!tx) mbar_arrive(&s_full[bt]);
       ++armed[bt];
       // once the compute warps are done with buffer bp (phase 2 of p, or just
@@ -241,17 +290,16 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
       }
       p2par[bp] ^= 1u;
       if (p != NONE) {
-        if (tma_ok) {
-          const uint32_t count = scan_tile_count<T>(n, p);
-          const uint64_t base = (uint64_t)p * TILE;
+        const ScanTile<T> tl = src.tile(p);
+        if (tl.tma) {
           const T *bP = buf(bp);
-          const uint32_t bulk = count & ~(uint32_t)(V - 1);
+          const uint32_t bulk = tl.count & ~(uint32_t)(V - 1);
           if (bulk > 0) {
-            tma_store_1d_hint(out + base, bP, bulk * (uint32_t)sizeof(T), stream);
+            tma_store_1d_hint(tl.out, bP, bulk * (uint32_t)sizeof(T), stream);
             tma_store_commit();
             issued_store = true;
           }
-          for (uint32_t i = bulk; i < count; ++i) out[base + i] = bP[i];
+          for (uint32_t i = bulk; i < tl.count; ++i) tl.out[i] = bP[i];
         }
       }
       p_tile = q_tile;
@@ -306,12 +354,13 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
       // publish their aggregates
       if (!wait_queued(j + 2u)) break;
       const T agg = s_q_agg[j % Q];
-      T excl = init;
+      const ScanTile<T> tl = src.tile(q);
+      T excl = tl.init;
       bool ok = true;
-      if (q != 0) ok = lookback_exclusive<T>(st, q, op, excl, hdr, spin_limit_ns);
+      if (!tl.first) ok = lookback_exclusive<T>(st, q, op, excl, hdr, spin_limit_ns);
       if (lane == 0) {
         if (ok) {
-          if (q != 0 && (long long)q != skip_publish_tile) st.publish(q, kStPrefix, op(excl, agg));
+          if (!tl.first && (long long)q != skip_publish_tile) st.publish(q, kStPrefix, op(excl, agg));
           s_q_prefix[j % Q] = excl;
           mbar_arrive(&s_qbar[j % Q]);
         } else {
@@ -341,20 +390,20 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
     bad = __any_sync(0xffffffffu, bad);  // warp-uniform, so the shuffles below never diverge
     if (!bad) t = s_ticket[bt];
     if (t != NONE) {
-      const uint32_t count = scan_tile_count<T>(n, t);
-      const uint64_t base = (uint64_t)t * TILE;
+      const ScanTile<T> tl = src.tile(t);
+      const uint32_t count = tl.count;
       const T *bT = buf(bt);
       T a = Op::identity();
 #pragma unroll
       for (int k = 0; k < R; ++k) {
         const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
         T x[V];
-        if (tma_ok) {
+        if (tl.tma) {
           const uint4 c = reinterpret_cast<const uint4 *>(bT)[elem / V];
           memcpy(&x[0], &c, 16);
         } else {
 #pragma unroll
-          for (int j = 0; j < V; ++j) x[j] = (elem + j < count) ? in[base + elem + j] : Op::identity();
+          for (int j = 0; j < V; ++j) x[j] = (elem + j < count) ? tl.in[elem + j] : Op::identity();
         }
 #pragma unroll
         for (int j = 0; j < V; ++j)
@@ -378,7 +427,8 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
 #pragma unroll
         for (int i = 1; i < kScanWarps; ++i) agg = op(agg, s_wtot[it & 3][i]);
         if ((long long)t != skip_publish_tile) {
-          if (t == 0) st.publish(0u, kStPrefix, op(init, agg));
+          const ScanTile<T> tl = src.tile(t);
+          if (tl.first) st.publish(t, kStPrefix, op(tl.init, agg));
           else st.publish(t, kStAggregate, agg);
         }
       }
@@ -396,8 +446,8 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
     }
     bad = __any_sync(0xffffffffu, bad);
     if (p != NONE && !bad) {
-      const uint32_t count = scan_tile_count<T>(n, p);
-      const uint64_t base = (uint64_t)p * TILE;
+      const ScanTile<T> tl = src.tile(p);
+      const uint32_t count = tl.count;
       T *const bP = buf(bp);
       const unsigned int e = (unsigned int)it - 2u;
       T before = s_q_prefix[e % Q];  // everything before this warp's first element
@@ -406,12 +456,12 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
 #pragma unroll
       for (int k = 0; k < R; ++k) {
         const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
-        if (tma_ok) {
+        if (tl.tma) {
           const uint4 c = reinterpret_cast<const uint4 *>(bP)[elem / V];
           memcpy(&y[k][0], &c, 16);
         } else {
 #pragma unroll
-          for (int j = 0; j < V; ++j) y[k][j] = (elem + j < count) ? in[base + elem + j] : Op::identity();
+          for (int j = 0; j < V; ++j) y[k][j] = (elem + j < count) ? tl.in[elem + j] : Op::identity();
         }
       }
 #pragma unroll
@@ -444,17 +494,17 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
         for (int j = 0; j < V; ++j) y[k][j] = op(b, y[k][j]);
         before = op(before, tot);
         const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
-        if (tma_ok) {
+        if (tl.tma) {
           uint4 c;
           memcpy(&c, &y[k][0], 16);
           reinterpret_cast<uint4 *>(bP)[elem / V] = c;
         } else {
 #pragma unroll
           for (int j = 0; j < V; ++j)
-            if (elem + j < count) out[base + elem + j] = y[k][j];
+            if (elem + j < count) tl.out[elem + j] = y[k][j];
         }
       }
-      if (tma_ok) fence_proxy_async_smem();
+      if (tl.tma) fence_proxy_async_smem();
     }
     __syncwarp();
     if (!bad && lane == 0) mbar_arrive(&s_p2[bp]);
@@ -465,40 +515,104 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const T *in, T *o
   }
 }
 
-template <typename T, typename Op>
-int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
+// Clears the status words, then runs the persistent scan over `tiles` tiles
+// of `src` (one array or a batch).
+template <typename T, typename Op, typename Src>
+int scan_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
   using C = ScanCfg<T>;
   host::DeviceInfo di;
   int st = host::device_info(&di);
   if (st != BK_OK) return st;
-  if (n == 0) return BK_OK;
-  if (d_in == nullptr || d_out == nullptr) return BK_ERR_INVALID_ARGUMENT;
-  if (!host::aligned_to<T>(d_in) || !host::aligned_to<T>(d_out)) return BK_ERR_MISALIGNED;
-  const size_t tiles = scan_num_tiles<T>(n);
   if (tiles >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
-  st = host::check_ws(d_ws, ws_bytes, scan_ws_bytes<T>(n));
+  st = host::check_ws(d_ws, ws_bytes, kHeaderBytes + C::Status::bytes(tiles));
   if (st != BK_OK) return st;
-
   WsHeader *hdr = reinterpret_cast<WsHeader *>(d_ws);
   auto status = scan_status_at<typename C::Status>(d_ws, tiles);
   const unsigned init_grid = (unsigned)std::min<size_t>((tiles + 255) / 256, (size_t)di.sm_count * 8);
   lookback_init_kernel<<<init_grid, 256, 0, stream>>>(status, tiles, hdr);
   st = host::launch_status();
   if (st != BK_OK) return st;
-
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
-  const int tma_ok = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15) == 0;
   const size_t smem = (size_t)kScanBufs * C::TILE_BYTES;
-  static thread_local bool attr_set = false;  // per host thread; cheap and idempotent
+  static thread_local bool attr_set = false;  // per host thread and kernel; cheap and idempotent
   if (!attr_set) {
-    if ((st = host::set_smem_attrs(scan_kernel<T, Op>, smem)) != BK_OK) return st;
+    if ((st = host::set_smem_attrs(scan_kernel<T, Op, Src>, smem)) != BK_OK) return st;
     attr_set = true;
   }
   const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * 2);
-  scan_kernel<T, Op><<<grid, kScanThreads, smem, stream>>>(d_in, d_out, n, init, status, hdr, limit,
-                                                           dbg.skip_publish_tile, tma_ok, (unsigned)tiles);
+  scan_kernel<T, Op, Src><<<grid, kScanThreads, smem, stream>>>(src, status, hdr, limit, dbg.skip_publish_tile,
+                                                                (unsigned)tiles);
   return host::launch_status();
+}
+
+template <typename T, typename Op>
+int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
+  if (n == 0) {
+    host::DeviceInfo di;
+    return host::device_info(&di);
+  }
+  if (d_in == nullptr || d_out == nullptr) return BK_ERR_INVALID_ARGUMENT;
+  if (!host::aligned_to<T>(d_in) || !host::aligned_to<T>(d_out)) return BK_ERR_MISALIGNED;
+  const int tma = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15) == 0;
+  const ScanOne<T> src{d_in, d_out, n, init, tma};
+  return scan_run<T, Op>(src, scan_num_tiles<T>(n), d_ws, ws_bytes, stream);
+}
+
+// A batch item as the C-ABI passes it (bk_scan_item_<type>).
+template <typename T>
+struct ScanItem {
+  const T *d_in;
+  T *d_out;
+  uint64_t n;
+  T init;
+};
+
+template <typename T>
+size_t scan_batch_tiles(const uint64_t *sizes, uint32_t count) {
+  size_t tiles = 0;
+  for (uint32_t i = 0; i < count; ++i) tiles += scan_num_tiles<T>(sizes[i]);
+  return tiles;
+}
+
+template <typename T, typename Op>
+int scan_batch_launch(const ScanItem<T> *items, uint32_t count, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
+  if (count > 0 && items == nullptr) return BK_ERR_INVALID_ARGUMENT;
+  if (count > (uint32_t)kScanBatchMax) return BK_ERR_TOO_LARGE;
+  ScanBatch<T> b;
+  b.count = 0;
+  size_t tiles = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const ScanItem<T> &it = items[i];
+    if (it.n == 0) continue;  // nothing to do; takes no tile
+    if (it.d_in == nullptr || it.d_out == nullptr) return BK_ERR_INVALID_ARGUMENT;
+    if (!host::aligned_to<T>(it.d_in) || !host::aligned_to<T>(it.d_out)) return BK_ERR_MISALIGNED;
+    const uint32_t k = b.count++;
+    b.in[k] = it.d_in;
+    b.out[k] = it.d_out;
+    b.n[k] = it.n;
+    b.init[k] = it.init;
+    b.start[k] = (uint32_t)tiles;
+    tiles += scan_num_tiles<T>(it.n);
+    if (tiles >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
+  }
+  b.start[b.count] = (uint32_t)tiles;
+  if (b.count == 0) {
+    host::DeviceInfo di;
+    return host::device_info(&di);
+  }
+  return scan_run<T, Op>(b, tiles, d_ws, ws_bytes, stream);
+}
+
+size_t scan_batch_workspace_bytes(int dtype, const uint64_t *sizes, uint32_t count) {
+  if (count > 0 && sizes == nullptr) return 0;
+  switch (dtype) {
+    case BK_DTYPE_I32: case BK_DTYPE_U32: case BK_DTYPE_F32:
+      return kHeaderBytes + ScanCfg<float>::Status::bytes(scan_batch_tiles<float>(sizes, count));
+    case BK_DTYPE_I64: case BK_DTYPE_U64: case BK_DTYPE_F64:
+      return kHeaderBytes + ScanCfg<double>::Status::bytes(scan_batch_tiles<double>(sizes, count));
+    default: return 0;
+  }
 }
 
 size_t scan_workspace_bytes(int dtype, uint64_t n) {
@@ -526,5 +640,20 @@ size_t scan_workspace_bytes(int dtype, uint64_t n) {
   BK_DEFINE_SCAN(OPNAME, OPT, f64, double)
 
 BK_DEFINE_SCAN_ALL_T(sum, OpSum)
+
+#define BK_DEFINE_SCAN_BATCH(TN, T)                                                                            \
+  static_assert(sizeof(bk_scan_item_##TN) == sizeof(bk::ScanItem<T>), "bk_scan_item layout");              \
+  extern "C" int bk_inclusive_scan_sum_##TN##_batch(const bk_scan_item_##TN *items, uint32_t count,          \
+                                                    void *d_ws, size_t ws_bytes, bk_stream_t stream) {       \
+    return bk::scan_batch_launch<T, bk::OpSum<T>>(reinterpret_cast<const bk::ScanItem<T> *>(items), count,   \
+                                                  d_ws, ws_bytes, (cudaStream_t)stream);                    \
+  }
+
+BK_DEFINE_SCAN_BATCH(i32, int32_t)
+BK_DEFINE_SCAN_BATCH(u32, uint32_t)
+BK_DEFINE_SCAN_BATCH(i64, int64_t)
+BK_DEFINE_SCAN_BATCH(u64, uint64_t)
+BK_DEFINE_SCAN_BATCH(f32, float)
+BK_DEFINE_SCAN_BATCH(f64, double)
 BK_DEFINE_SCAN_ALL_T(min, OpMin)
 BK_DEFINE_SCAN_ALL_T(max, OpMax)

@@ -73,6 +73,11 @@ BK_API const char *bk_status_string(int status);
  * Returns 0 for an unknown combination. */
 BK_API size_t bk_workspace_bytes(int algo, int key_dtype, int value_dtype, uint64_t n);
 
+/* Bytes of device workspace that one batched call (the *_batch entry points
+ * below) of `algo` over `count` arrays needs; sizes[i] (host memory) is the
+ * element count of array i.  Returns 0 for an unknown combination. */
+BK_API size_t bk_batch_workspace_bytes(int algo, int key_dtype, int value_dtype, const uint64_t *sizes, uint32_t count);
+
 /* Zero-fill a workspace on `stream` (the one-time initialisation). */
 BK_API int bk_workspace_init(void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
@@ -222,6 +227,56 @@ BK_API int bk_reduce_by_key_i64_f64(const int64_t *keys, const double *vals, uin
  * GPU (concurrent streams, other threads) race and corrupt each other, so
  * serialise them.  Device-side wait errors are not reported by this variant. */
 BK_API int bk_inclusive_scan_sum_f32_noalloc(const float *d_in, uint64_t n, float init, float *d_out, bk_stream_t stream);
+
+/* ---- batched entry points --------------------------------------------------
+ * No counterpart in the reference, whose drivers launch once per array.  One
+ * call processes up to BK_BATCH_MAX independent arrays with a single
+ * persistent launch (plus one small initialisation kernel): every array's
+ * result is exactly what the single-array entry point gives for it, and the
+ * GPU stays full even when each array is small.  `items` is in host memory;
+ * items with n == 0 are skipped.  Workspace: bk_batch_workspace_bytes over
+ * the items' sizes, same contract as above. */
+#define BK_BATCH_MAX 256
+
+typedef struct bk_scan_item_i32 { const int32_t *d_in; int32_t *d_out; uint64_t n; int32_t init; } bk_scan_item_i32;
+typedef struct bk_scan_item_u32 { const uint32_t *d_in; uint32_t *d_out; uint64_t n; uint32_t init; } bk_scan_item_u32;
+typedef struct bk_scan_item_i64 { const int64_t *d_in; int64_t *d_out; uint64_t n; int64_t init; } bk_scan_item_i64;
+typedef struct bk_scan_item_u64 { const uint64_t *d_in; uint64_t *d_out; uint64_t n; uint64_t init; } bk_scan_item_u64;
+typedef struct bk_scan_item_f32 { const float *d_in; float *d_out; uint64_t n; float init; } bk_scan_item_f32;
+typedef struct bk_scan_item_f64 { const double *d_in; double *d_out; uint64_t n; double init; } bk_scan_item_f64;
+
+/* Inclusive sum scans of up to BK_BATCH_MAX arrays: for each item,
+ * d_out[i] = init + d_in[0] + ... + d_in[i] (as bk_inclusive_scan_sum_*). */
+BK_API int bk_inclusive_scan_sum_i32_batch(const bk_scan_item_i32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_u32_batch(const bk_scan_item_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_i64_batch(const bk_scan_item_i64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_u64_batch(const bk_scan_item_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_f32_batch(const bk_scan_item_f32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_f64_batch(const bk_scan_item_f64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
+/* reduce_by_key of up to BK_BATCH_MAX arrays: for each item, the runs of
+ * its keys go to its out_keys / out_vals and their count to its d_num_out
+ * (as bk_reduce_by_key_*). */
+typedef struct bk_rbk_item_i32_i32 { const int32_t *keys; const int32_t *vals; uint64_t n; int32_t *out_keys; int32_t *out_vals; uint64_t *d_num_out; } bk_rbk_item_i32_i32;
+typedef struct bk_rbk_item_i32_i64 { const int32_t *keys; const int64_t *vals; uint64_t n; int32_t *out_keys; int64_t *out_vals; uint64_t *d_num_out; } bk_rbk_item_i32_i64;
+typedef struct bk_rbk_item_i32_f32 { const int32_t *keys; const float *vals; uint64_t n; int32_t *out_keys; float *out_vals; uint64_t *d_num_out; } bk_rbk_item_i32_f32;
+typedef struct bk_rbk_item_i32_f64 { const int32_t *keys; const double *vals; uint64_t n; int32_t *out_keys; double *out_vals; uint64_t *d_num_out; } bk_rbk_item_i32_f64;
+typedef struct bk_rbk_item_u32_f32 { const uint32_t *keys; const float *vals; uint64_t n; uint32_t *out_keys; float *out_vals; uint64_t *d_num_out; } bk_rbk_item_u32_f32;
+typedef struct bk_rbk_item_u32_f64 { const uint32_t *keys; const double *vals; uint64_t n; uint32_t *out_keys; double *out_vals; uint64_t *d_num_out; } bk_rbk_item_u32_f64;
+typedef struct bk_rbk_item_i64_i32 { const int64_t *keys; const int32_t *vals; uint64_t n; int64_t *out_keys; int32_t *out_vals; uint64_t *d_num_out; } bk_rbk_item_i64_i32;
+typedef struct bk_rbk_item_i64_i64 { const int64_t *keys; const int64_t *vals; uint64_t n; int64_t *out_keys; int64_t *out_vals; uint64_t *d_num_out; } bk_rbk_item_i64_i64;
+typedef struct bk_rbk_item_i64_f32 { const int64_t *keys; const float *vals; uint64_t n; int64_t *out_keys; float *out_vals; uint64_t *d_num_out; } bk_rbk_item_i64_f32;
+typedef struct bk_rbk_item_i64_f64 { const int64_t *keys; const double *vals; uint64_t n; int64_t *out_keys; double *out_vals; uint64_t *d_num_out; } bk_rbk_item_i64_f64;
+BK_API int bk_reduce_by_key_i32_i32_batch(const bk_rbk_item_i32_i32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i32_i64_batch(const bk_rbk_item_i32_i64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i32_f32_batch(const bk_rbk_item_i32_f32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i32_f64_batch(const bk_rbk_item_i32_f64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_u32_f32_batch(const bk_rbk_item_u32_f32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_u32_f64_batch(const bk_rbk_item_u32_f64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i64_i32_batch(const bk_rbk_item_i64_i32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i64_i64_batch(const bk_rbk_item_i64_i64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i64_f32_batch(const bk_rbk_item_i64_f32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_reduce_by_key_i64_f64_batch(const bk_rbk_item_i64_f64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
 #ifdef __cplusplus
 } /* extern "C" */
