@@ -18,6 +18,12 @@ from .algorithms import (  # noqa: F401
     workspaces,
 )
 
-from .batch import BATCH_MAX, batch_workspace_bytes, inclusive_scan_batch, reduce_by_key_batch  # noqa: F401
+from .batch import (  # noqa: F401
+    BATCH_MAX,
+    batch_workspace_bytes,
+    inclusive_scan_batch,
+    reduce_by_key_batch,
+    stable_sort_by_key_batch,
+)
 
 __version__ = "1.0.0"

@@ -43,6 +43,13 @@ def rbk_item_type(key: str, value: str):
                               ("d_num_out", ctypes.c_void_p)]})
 
 
+@lru_cache(maxsize=None)
+def sort_item_type(key: str, value: str):
+    """ctypes mirror of bk_sort_item_<key>_<value>."""
+    return type(f"bk_sort_item_{key}_{value}", (ctypes.Structure,),
+                {"_fields_": [("keys", ctypes.c_void_p), ("vals", ctypes.c_void_p), ("n", ctypes.c_uint64)]})
+
+
 def batch_workspace_bytes(algo: str, key: str, value: str | None, sizes) -> int:
     arr = (ctypes.c_uint64 * max(len(sizes), 1))(*sizes)
     return lib.bk_batch_workspace_bytes(_lib.ALGO[algo], _lib.DTYPE[key], _lib.DTYPE[value], arr, len(sizes))
@@ -122,3 +129,36 @@ def reduce_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | None =
         return [(ok, ov, counts[i:i + 1]) for i, (ok, ov) in enumerate(res)]
     cs = counts.tolist()
     return [(ok[:c], ov[:c], c) for (ok, ov), c in zip(res, cs)]
+
+
+def stable_sort_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | None = None):
+    """Stable sort of every (keys, vals) pair in place (payloads of 4 or 8
+    bytes, passed through unchanged).  Returns the lists."""
+    keys_list, vals_list = list(keys_list), list(vals_list)
+    if len(keys_list) != len(vals_list):
+        raise ValueError("keys_list and vals_list must have the same length")
+    if not keys_list:
+        return keys_list, vals_list
+    dev = _require_cuda(*keys_list, *vals_list)
+    kt = dtype_tag(keys_list[0].dtype)
+    vsize = vals_list[0].element_size()
+    if vsize not in (4, 8):
+        raise TypeError("payloads must be 4 or 8 bytes")
+    vt = "u32" if vsize == 4 else "u64"
+    for k, v in zip(keys_list, vals_list):
+        if dtype_tag(k.dtype) != kt or v.element_size() != vsize:
+            raise TypeError("one key dtype and one payload size per batch")
+        if k.numel() != v.numel():
+            raise ValueError("keys and vals must have the same length")
+    s = _stream_handle(stream, dev)
+    item_t = sort_item_type(kt, vt)
+    fn = getattr(lib, f"bk_sort_by_key_{kt}_{vt}_batch")
+    for lo, hi in _chunks(len(keys_list)):
+        items = (item_t * (hi - lo))()
+        for j, i in enumerate(range(lo, hi)):
+            items[j].keys, items[j].vals, items[j].n = keys_list[i].data_ptr(), vals_list[i].data_ptr(), \
+                keys_list[i].numel()
+        need = batch_workspace_bytes("sort_by_key", kt, vt, [keys_list[i].numel() for i in range(lo, hi)])
+        ws, wsb = workspaces.get(max(need, 256), dev, s)
+        check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
+    return keys_list, vals_list

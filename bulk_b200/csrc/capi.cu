@@ -14,6 +14,7 @@ size_t sort_workspace_bytes(int key_dtype, int value_dtype, uint64_t n);
 size_t rbk_workspace_bytes(int key_dtype, int value_dtype, uint64_t n);
 size_t scan_batch_workspace_bytes(int dtype, const uint64_t *sizes, uint32_t count);
 size_t rbk_batch_workspace_bytes(int key_dtype, int value_dtype, const uint64_t *sizes, uint32_t count);
+size_t sort_batch_workspace_bytes(int key_dtype, int value_dtype, const uint64_t *sizes, uint32_t count);
 
 namespace host {
 
@@ -88,6 +89,7 @@ extern "C" size_t bk_batch_workspace_bytes(int algo, int key_dtype, int value_dt
     case BK_ALGO_INCLUSIVE_SCAN:
       return value_dtype == BK_DTYPE_NONE ? bk::scan_batch_workspace_bytes(key_dtype, sizes, count) : 0;
     case BK_ALGO_REDUCE_BY_KEY: return bk::rbk_batch_workspace_bytes(key_dtype, value_dtype, sizes, count);
+    case BK_ALGO_SORT_BY_KEY: return bk::sort_batch_workspace_bytes(key_dtype, value_dtype, sizes, count);
     default: return 0;
   }
 }

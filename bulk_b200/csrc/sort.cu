@@ -41,16 +41,77 @@ constexpr size_t mp_smem_bytes() {
          (size_t)payload_bytes<P>() * padded_len(SortCfg<K>::MP_TILE);
 }
 
-// Stable sort of one tile: in -> out (may alias).
+// A block-sort tile: `count` elements from in_* to out_* (may alias), both
+// already offset to the tile.
 template <typename K, typename P>
-__global__ void __launch_bounds__(kBsThreads) block_sort_kernel(const K *in_k, const P *in_v, K *out_k, P *out_v,
-                                                                uint64_t n) {
+struct BsTile {
+  const K *in_k;
+  const P *in_v;
+  K *out_k;
+  P *out_v;
+  int count;
+};
+
+// Block-sort tiles of one array.
+template <typename K, typename P>
+struct BsOne {
+  const K *in_k;
+  const P *in_v;
+  K *out_k;
+  P *out_v;
+  uint64_t n;
+  __device__ __forceinline__ BsTile<K, P> tile(unsigned int t) const {
+    const uint64_t base = (uint64_t)t * SortCfg<K>::BS_TILE;
+    const int count = (int)((n - base) < (uint64_t)SortCfg<K>::BS_TILE ? (n - base) : (uint64_t)SortCfg<K>::BS_TILE);
+    return BsTile<K, P>{in_k + base, has_payload<P>() ? in_v + base : nullptr, out_k + base,
+                        has_payload<P>() ? out_v + base : nullptr, count};
+  }
+};
+
+// Finds the batch item owning global tile t: the last i with start[i] <= t.
+__device__ __forceinline__ int batch_item_of(const uint32_t *start, uint32_t count, unsigned int t) {
+  int lo = 0, hi = (int)count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+constexpr int kSortBatchMax = 256;
+
+// Block-sort tiles of a batch of arrays (array i owns global tiles
+// [start[i], start[i + 1])); the descriptors travel in the kernel parameters.
+template <typename K, typename P>
+struct BsBatch {
+  const K *in_k[kSortBatchMax];
+  const P *in_v[kSortBatchMax];
+  K *out_k[kSortBatchMax];
+  P *out_v[kSortBatchMax];
+  uint64_t n[kSortBatchMax];
+  uint32_t start[kSortBatchMax + 1];
+  uint32_t count;
+  __device__ __forceinline__ BsTile<K, P> tile(unsigned int t) const {
+    const int i = batch_item_of(start, count, t);
+    const uint64_t base = (uint64_t)(t - start[i]) * SortCfg<K>::BS_TILE;
+    const int cnt = (int)((n[i] - base) < (uint64_t)SortCfg<K>::BS_TILE ? (n[i] - base) : (uint64_t)SortCfg<K>::BS_TILE);
+    return BsTile<K, P>{in_k[i] + base, has_payload<P>() ? in_v[i] + base : nullptr, out_k[i] + base,
+                        has_payload<P>() ? out_v[i] + base : nullptr, cnt};
+  }
+};
+
+// Stable sort of one tile: in -> out (may alias).
+template <typename K, typename P, typename Src>
+__global__ void __launch_bounds__(kBsThreads) block_sort_kernel(const __grid_constant__ Src src) {
   constexpr int ITEMS = SortCfg<K>::BS_ITEMS, TILE = SortCfg<K>::BS_TILE;
   extern __shared__ __align__(16) unsigned char smem[];
   K *sk = reinterpret_cast<K *>(smem);
   P *sv = reinterpret_cast<P *>(smem + align_up(sizeof(K) * padded_len(TILE), 16));  // padded layout
-  const uint64_t base = (uint64_t)blockIdx.x * TILE;
-  const int count = (int)((n - base) < (uint64_t)TILE ? (n - base) : (uint64_t)TILE);
+  const BsTile<K, P> tl = src.tile(blockIdx.x);
+  const K *in_k = tl.in_k;
+  const P *in_v = tl.in_v;
+  const int count = tl.count;
   const int tid = threadIdx.x;
 
   // stage in (all loads in flight before the first store); pad a partial
@@ -60,14 +121,14 @@ __global__ void __launch_bounds__(kBsThreads) block_sort_kernel(const K *in_k, c
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
       const int i = j * kBsThreads + tid;
-      tk[j] = i < count ? __ldg(in_k + base + i) : key_max<K>();
+      tk[j] = i < count ? __ldg(in_k + i) : key_max<K>();
     }
     if constexpr (has_payload<P>()) {
       P tv[ITEMS];
 #pragma unroll
       for (int j = 0; j < ITEMS; ++j) {
         const int i = j * kBsThreads + tid;
-        tv[j] = i < count ? __ldg(in_v + base + i) : P();
+        tv[j] = i < count ? __ldg(in_v + i) : P();
       }
 #pragma unroll
       for (int j = 0; j < ITEMS; ++j) sv[pad32(j * kBsThreads + tid)] = tv[j];
@@ -126,31 +187,79 @@ __global__ void __launch_bounds__(kBsThreads) block_sort_kernel(const K *in_k, c
     if constexpr (has_payload<P>()) sv[pad32(tid * ITEMS + i)] = v[i];
   }
   __syncthreads();
-  stage_out_padded<kBsThreads>(out_k + base, sk, count);
-  if constexpr (has_payload<P>()) stage_out_padded<kBsThreads>(out_v + base, sv, count);
+  stage_out_padded<kBsThreads>(tl.out_k, sk, count);
+  if constexpr (has_payload<P>()) stage_out_padded<kBsThreads>(tl.out_v, sv, count);
 }
 
-// Merge pass: runs of width w in `src` -> runs of 2w in `dst`.
-// parts[t] = A-split of output tile t at its diagonal inside its pair.
-template <typename K>
-__global__ void sort_partition_kernel(const K *keys, uint64_t n, uint64_t w, uint64_t num_tiles, uint64_t *parts) {
-  constexpr uint64_t T = SortCfg<K>::MP_TILE;
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= num_tiles) return;
-  const uint64_t d = t * T;
-  const uint64_t p0 = d / (2 * w) * (2 * w);
-  const uint64_t a_end = p0 + w < n ? p0 + w : n;
-  const uint64_t b_end = p0 + 2 * w < n ? p0 + 2 * w : n;
-  parts[t] = merge_path<K, uint64_t>(keys + p0, a_end - p0, keys + a_end, b_end - a_end, d - p0);
-}
+// A merge-pass tile: output tile `local` of a pass over one array that
+// merges runs of width w in src_* into runs of 2w in dst_*; parts[t] is the
+// A-split of the array's output tile t at its diagonal inside its pair.
+template <typename K, typename P>
+struct MpTile {
+  const K *src_k;
+  const P *src_v;
+  K *dst_k;
+  P *dst_v;
+  uint64_t n;
+  uint64_t w;
+  uint64_t *parts;
+  uint64_t local;
+  uint64_t num_tiles;
+};
 
 template <typename K, typename P>
-__global__ void __launch_bounds__(kMpThreads, 4) sort_merge_kernel(const K *sk, const P *sv, K *dk, P *dv, uint64_t n,
-                                                                uint64_t w, const uint64_t *parts,
-                                                                uint64_t num_tiles) {
+struct MpOne {
+  const K *src_k;
+  const P *src_v;
+  K *dst_k;
+  P *dst_v;
+  uint64_t n;
+  uint64_t w;
+  uint64_t *parts;
+  uint64_t num_tiles;
+  __device__ __forceinline__ MpTile<K, P> tile(uint64_t t) const {
+    return MpTile<K, P>{src_k, src_v, dst_k, dst_v, n, w, parts, t, num_tiles};
+  }
+};
+
+// One merge pass over a batch of arrays (only those that still need it).
+template <typename K, typename P>
+struct MpBatch {
+  const K *src_k[kSortBatchMax];
+  const P *src_v[kSortBatchMax];
+  K *dst_k[kSortBatchMax];
+  P *dst_v[kSortBatchMax];
+  uint64_t n[kSortBatchMax];
+  uint64_t *parts[kSortBatchMax];
+  uint32_t start[kSortBatchMax + 1];
+  uint64_t w;
+  uint32_t count;
+  __device__ __forceinline__ MpTile<K, P> tile(uint64_t t) const {
+    const int i = batch_item_of(start, count, (unsigned int)t);
+    return MpTile<K, P>{src_k[i], src_v[i], dst_k[i], dst_v[i], n[i], w, parts[i], t - start[i],
+                        (uint64_t)(start[i + 1] - start[i])};
+  }
+};
+
+template <typename K, typename P, typename Src>
+__global__ void sort_partition_kernel(const __grid_constant__ Src src, uint64_t total_tiles) {
+  constexpr uint64_t T = SortCfg<K>::MP_TILE;
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total_tiles) return;
+  const MpTile<K, P> m = src.tile(g);
+  const uint64_t d = m.local * T;
+  const uint64_t p0 = d / (2 * m.w) * (2 * m.w);
+  const uint64_t a_end = p0 + m.w < m.n ? p0 + m.w : m.n;
+  const uint64_t b_end = p0 + 2 * m.w < m.n ? p0 + 2 * m.w : m.n;
+  m.parts[m.local] = merge_path<K, uint64_t>(m.src_k + p0, a_end - p0, m.src_k + a_end, b_end - a_end, d - p0);
+}
+
+template <typename K, typename P, typename Src>
+__global__ void __launch_bounds__(kMpThreads, 4) sort_merge_kernel(const __grid_constant__ Src src) {
   constexpr uint64_t T = SortCfg<K>::MP_TILE;
   extern __shared__ __align__(16) unsigned char smem[];
-  const uint64_t t = blockIdx.x;
+  const MpTile<K, P> m = src.tile(blockIdx.x);
+  const uint64_t t = m.local, n = m.n, w = m.w;
   const uint64_t d = t * T;
   const uint64_t p0 = d / (2 * w) * (2 * w);
   const uint64_t a_end = p0 + w < n ? p0 + w : n;
@@ -158,14 +267,16 @@ __global__ void __launch_bounds__(kMpThreads, 4) sort_merge_kernel(const K *sk, 
   const uint64_t la_all = a_end - p0, lb_all = b_end - a_end;
   const uint64_t diag0 = d - p0;
   const uint64_t diag1 = (diag0 + T < la_all + lb_all) ? diag0 + T : la_all + lb_all;
-  const uint64_t a0 = parts[t];
+  const uint64_t a0 = m.parts[t];
   // the next tile's split belongs to this pair only if it starts inside it
-  const uint64_t a1 = (t + 1 < num_tiles && d + T < b_end) ? parts[t + 1] : la_all;
+  const uint64_t a1 = (t + 1 < m.num_tiles && d + T < b_end) ? m.parts[t + 1] : la_all;
   const uint64_t b0 = diag0 - a0, b1 = diag1 - a1;
+  const K *sk = m.src_k;
+  const P *sv = m.src_v;
   merge_tile<kMpThreads, SortCfg<K>::MP_ITEMS, K, P>(
       sk + p0 + a0, has_payload<P>() ? sv + p0 + a0 : nullptr, (int)(a1 - a0), sk + a_end + b0,
-      has_payload<P>() ? sv + a_end + b0 : nullptr, (int)(b1 - b0), dk + d, has_payload<P>() ? dv + d : nullptr,
-      smem);
+      has_payload<P>() ? sv + a_end + b0 : nullptr, (int)(b1 - b0), m.dst_k + d,
+      has_payload<P>() ? m.dst_v + d : nullptr, smem);
 }
 
 template <typename K, typename P>
@@ -180,6 +291,36 @@ static int set_smem(Kern kern, size_t bytes) {
   return host::set_smem_attrs(kern, bytes);
 }
 
+template <typename K>
+int sort_passes(uint64_t n) {
+  int passes = 0;
+  for (uint64_t w = SortCfg<K>::BS_TILE; w < n; w *= 2) ++passes;
+  return passes;
+}
+
+template <typename K, typename P, typename BsSrc, typename MpSrc>
+int sort_set_attrs() {
+  static thread_local bool attr_set = false;
+  if (!attr_set) {
+    int st;
+    if ((st = set_smem(block_sort_kernel<K, P, BsSrc>, bs_smem_bytes<K, P>())) != BK_OK) return st;
+    if ((st = set_smem(sort_merge_kernel<K, P, MpSrc>, mp_smem_bytes<K, P>())) != BK_OK) return st;
+    attr_set = true;
+  }
+  return BK_OK;
+}
+
+template <typename K, typename P>
+int sort_check_array(K *keys, P *vals, uint64_t n) {
+  if (n > 0 && (keys == nullptr || (has_payload<P>() && vals == nullptr))) return BK_ERR_INVALID_ARGUMENT;
+  if (!host::aligned_to<K>(keys)) return BK_ERR_MISALIGNED;
+  if constexpr (has_payload<P>()) {
+    if (!host::aligned_to<P>(vals)) return BK_ERR_MISALIGNED;
+  }
+  if ((n + SortCfg<K>::MP_TILE - 1) / SortCfg<K>::MP_TILE >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
+  return BK_OK;
+}
+
 template <typename K, typename P>
 int sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
   using C = SortCfg<K>;
@@ -187,14 +328,9 @@ int sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaS
   int st = host::device_info(&di);
   if (st != BK_OK) return st;
   if (n <= 1) return BK_OK;
-  if (keys == nullptr || (has_payload<P>() && vals == nullptr)) return BK_ERR_INVALID_ARGUMENT;
-  if (!host::aligned_to<K>(keys)) return BK_ERR_MISALIGNED;
-  if constexpr (has_payload<P>()) {
-    if (!host::aligned_to<P>(vals)) return BK_ERR_MISALIGNED;
-  }
+  if ((st = sort_check_array(keys, vals, n)) != BK_OK) return st;
   const uint64_t bs_tiles = (n + C::BS_TILE - 1) / C::BS_TILE;
   const uint64_t mp_tiles = (n + C::MP_TILE - 1) / C::MP_TILE;
-  if (mp_tiles >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
   st = host::check_ws(d_ws, ws_bytes, sort_ws_bytes_t<K, P>(n));
   if (st != BK_OK) return st;
   char *ws = reinterpret_cast<char *>(d_ws) + kHeaderBytes;
@@ -203,33 +339,157 @@ int sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaS
   P *tv = reinterpret_cast<P *>(ws);
   ws += align_up(n * (size_t)payload_bytes<P>(), 256);
   uint64_t *parts = reinterpret_cast<uint64_t *>(ws);
-
-  int passes = 0;
-  for (uint64_t w = C::BS_TILE; w < n; w *= 2) ++passes;
-
-  static thread_local bool attr_set = false;
-  if (!attr_set) {
-    if ((st = set_smem(block_sort_kernel<K, P>, bs_smem_bytes<K, P>())) != BK_OK) return st;
-    if ((st = set_smem(sort_merge_kernel<K, P>, mp_smem_bytes<K, P>())) != BK_OK) return st;
-    attr_set = true;
-  }
+  const int passes = sort_passes<K>(n);
+  if ((st = sort_set_attrs<K, P, BsOne<K, P>, MpOne<K, P>>()) != BK_OK) return st;
   // an odd number of passes starts in the temporaries so the last lands in place
   K *ck = (passes & 1) ? tk : keys;
   P *cv = (passes & 1) ? tv : vals;
-  block_sort_kernel<K, P><<<(unsigned)bs_tiles, kBsThreads, bs_smem_bytes<K, P>(), stream>>>(keys, vals, ck, cv, n);
+  block_sort_kernel<K, P, BsOne<K, P>><<<(unsigned)bs_tiles, kBsThreads, bs_smem_bytes<K, P>(), stream>>>(
+      BsOne<K, P>{keys, vals, ck, cv, n});
   if ((st = host::launch_status()) != BK_OK) return st;
   for (uint64_t w = C::BS_TILE; w < n; w *= 2) {
     K *nk = (ck == keys) ? tk : keys;
     P *nv = (ck == keys) ? tv : vals;
-    sort_partition_kernel<K><<<(unsigned)((mp_tiles + 255) / 256), 256, 0, stream>>>(ck, n, w, mp_tiles, parts);
+    const MpOne<K, P> src{ck, cv, nk, nv, n, w, parts, mp_tiles};
+    sort_partition_kernel<K, P, MpOne<K, P>><<<(unsigned)((mp_tiles + 255) / 256), 256, 0, stream>>>(src, mp_tiles);
     if ((st = host::launch_status()) != BK_OK) return st;
-    sort_merge_kernel<K, P><<<(unsigned)mp_tiles, kMpThreads, mp_smem_bytes<K, P>(), stream>>>(ck, cv, nk, nv, n, w,
-                                                                                             parts, mp_tiles);
+    sort_merge_kernel<K, P, MpOne<K, P>><<<(unsigned)mp_tiles, kMpThreads, mp_smem_bytes<K, P>(), stream>>>(src);
     if ((st = host::launch_status()) != BK_OK) return st;
     ck = nk;
     cv = nv;
   }
   return BK_OK;
+}
+
+// A batch item as the C-ABI passes it (bk_sort_item_<key>_<payload>).
+template <typename K, typename P>
+struct SortItem {
+  K *keys;
+  P *vals;
+  uint64_t n;
+};
+
+// Workspace of a batch: per array (n > 1), its key and payload temporaries
+// and its merge-pass splits, one after another.
+template <typename K, typename P>
+size_t sort_batch_ws_bytes_t(const uint64_t *sizes, uint32_t count) {
+  size_t b = kHeaderBytes;
+  for (uint32_t i = 0; i < count; ++i) {
+    const uint64_t n = sizes[i];
+    if (n <= 1) continue;
+    const uint64_t mp_tiles = (n + SortCfg<K>::MP_TILE - 1) / SortCfg<K>::MP_TILE;
+    b += align_up(n * sizeof(K), 256) + align_up(n * (size_t)payload_bytes<P>(), 256) +
+         align_up((mp_tiles + 1) * sizeof(uint64_t), 256);
+  }
+  return b;
+}
+
+template <typename K, typename P>
+int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
+  using C = SortCfg<K>;
+  if (count > 0 && items == nullptr) return BK_ERR_INVALID_ARGUMENT;
+  if (count > (uint32_t)kSortBatchMax) return BK_ERR_TOO_LARGE;
+  host::DeviceInfo di;
+  int st = host::device_info(&di);
+  if (st != BK_OK) return st;
+  // the arrays that need sorting, with their temporaries
+  struct Arr {
+    K *keys;
+    P *vals;
+    uint64_t n;
+    K *tk;
+    P *tv;
+    uint64_t *parts;
+    int passes;
+  };
+  Arr arr[kSortBatchMax];
+  uint32_t na = 0;
+  uint64_t sizes[kSortBatchMax];
+  for (uint32_t i = 0; i < count; ++i) {
+    if ((st = sort_check_array(items[i].keys, items[i].vals, items[i].n)) != BK_OK) return st;
+    sizes[i] = items[i].n;
+  }
+  st = host::check_ws(d_ws, ws_bytes, sort_batch_ws_bytes_t<K, P>(sizes, count));
+  if (st != BK_OK) return st;
+  char *ws = reinterpret_cast<char *>(d_ws) + kHeaderBytes;
+  int max_passes = 0;
+  size_t bs_total = 0;
+  BsBatch<K, P> bs;
+  bs.count = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const uint64_t n = items[i].n;
+    if (n <= 1) continue;  // already sorted
+    Arr &a = arr[na++];
+    a.keys = items[i].keys;
+    a.vals = items[i].vals;
+    a.n = n;
+    a.tk = reinterpret_cast<K *>(ws);
+    ws += align_up(n * sizeof(K), 256);
+    a.tv = reinterpret_cast<P *>(ws);
+    ws += align_up(n * (size_t)payload_bytes<P>(), 256);
+    a.parts = reinterpret_cast<uint64_t *>(ws);
+    ws += align_up(((n + C::MP_TILE - 1) / C::MP_TILE + 1) * sizeof(uint64_t), 256);
+    a.passes = sort_passes<K>(n);
+    max_passes = a.passes > max_passes ? a.passes : max_passes;
+    // an odd number of passes starts in the temporaries so the last lands in place
+    const uint32_t k = bs.count++;
+    bs.in_k[k] = a.keys;
+    bs.in_v[k] = a.vals;
+    bs.out_k[k] = (a.passes & 1) ? a.tk : a.keys;
+    bs.out_v[k] = (a.passes & 1) ? a.tv : a.vals;
+    bs.n[k] = n;
+    bs.start[k] = (uint32_t)bs_total;
+    bs_total += (n + C::BS_TILE - 1) / C::BS_TILE;
+  }
+  if (na == 0) return BK_OK;
+  bs.start[bs.count] = (uint32_t)bs_total;
+  if (bs_total >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
+  if ((st = sort_set_attrs<K, P, BsBatch<K, P>, MpBatch<K, P>>()) != BK_OK) return st;
+  block_sort_kernel<K, P, BsBatch<K, P>><<<(unsigned)bs_total, kBsThreads, bs_smem_bytes<K, P>(), stream>>>(bs);
+  if ((st = host::launch_status()) != BK_OK) return st;
+  // pass p merges runs of width BS_TILE << p for every array with more than p passes
+  for (int p = 0; p < max_passes; ++p) {
+    MpBatch<K, P> mp;
+    mp.count = 0;
+    mp.w = (uint64_t)C::BS_TILE << p;
+    size_t mp_total = 0;
+    for (uint32_t j = 0; j < na; ++j) {
+      const Arr &a = arr[j];
+      if (a.passes <= p) continue;
+      // after the block sort the data is in the temporaries iff passes is odd;
+      // each pass moves it to the other buffer
+      const bool from_tmp = ((a.passes - p) & 1) != 0;
+      const uint32_t k = mp.count++;
+      mp.src_k[k] = from_tmp ? a.tk : a.keys;
+      mp.src_v[k] = from_tmp ? a.tv : a.vals;
+      mp.dst_k[k] = from_tmp ? a.keys : a.tk;
+      mp.dst_v[k] = from_tmp ? a.vals : a.tv;
+      mp.n[k] = a.n;
+      mp.parts[k] = a.parts;
+      mp.start[k] = (uint32_t)mp_total;
+      mp_total += (a.n + C::MP_TILE - 1) / C::MP_TILE;
+    }
+    mp.start[mp.count] = (uint32_t)mp_total;
+    if (mp_total >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
+    sort_partition_kernel<K, P, MpBatch<K, P>><<<(unsigned)((mp_total + 255) / 256), 256, 0, stream>>>(mp, mp_total);
+    if ((st = host::launch_status()) != BK_OK) return st;
+    sort_merge_kernel<K, P, MpBatch<K, P>><<<(unsigned)mp_total, kMpThreads, mp_smem_bytes<K, P>(), stream>>>(mp);
+    if ((st = host::launch_status()) != BK_OK) return st;
+  }
+  return BK_OK;
+}
+
+size_t sort_batch_workspace_bytes(int key_dtype, int value_dtype, const uint64_t *sizes, uint32_t count) {
+  if (count > 0 && sizes == nullptr) return 0;
+  const bool k4 = key_dtype == BK_DTYPE_I32 || key_dtype == BK_DTYPE_U32 || key_dtype == BK_DTYPE_F32;
+  const bool k8 = key_dtype == BK_DTYPE_I64 || key_dtype == BK_DTYPE_U64 || key_dtype == BK_DTYPE_F64;
+  const bool v4 = value_dtype == BK_DTYPE_I32 || value_dtype == BK_DTYPE_U32 || value_dtype == BK_DTYPE_F32;
+  const bool v8 = value_dtype == BK_DTYPE_I64 || value_dtype == BK_DTYPE_U64 || value_dtype == BK_DTYPE_F64;
+  if (k4) return v4 ? sort_batch_ws_bytes_t<float, uint32_t>(sizes, count)
+                 : v8 ? sort_batch_ws_bytes_t<float, unsigned long long>(sizes, count) : 0;
+  if (k8) return v4 ? sort_batch_ws_bytes_t<double, uint32_t>(sizes, count)
+                 : v8 ? sort_batch_ws_bytes_t<double, unsigned long long>(sizes, count) : 0;
+  return 0;
 }
 
 size_t sort_workspace_bytes(int key_dtype, int value_dtype, uint64_t n) {
@@ -267,3 +527,21 @@ BK_DEFINE_SORT(i64, int64_t)
 BK_DEFINE_SORT(u64, uint64_t)
 BK_DEFINE_SORT(f32, float)
 BK_DEFINE_SORT(f64, double)
+
+#define BK_DEFINE_SORT_BATCH(KN, K, VN, V, VI)                                                                  \
+  static_assert(sizeof(bk_sort_item_##KN##_##VN) == sizeof(bk::SortItem<K, VI>), "bk_sort_item layout");     \
+  extern "C" int bk_sort_by_key_##KN##_##VN##_batch(const bk_sort_item_##KN##_##VN *items, uint32_t count,    \
+                                                    void *d_ws, size_t ws_bytes, bk_stream_t stream) {       \
+    return bk::sort_batch_launch<K, VI>(reinterpret_cast<const bk::SortItem<K, VI> *>(items), count, d_ws,    \
+                                        ws_bytes, (cudaStream_t)stream);                                      \
+  }
+#define BK_DEFINE_SORT_BATCH_K(KN, K)                                 \
+  BK_DEFINE_SORT_BATCH(KN, K, u32, uint32_t, uint32_t)                \
+  BK_DEFINE_SORT_BATCH(KN, K, u64, uint64_t, unsigned long long)
+
+BK_DEFINE_SORT_BATCH_K(i32, int32_t)
+BK_DEFINE_SORT_BATCH_K(u32, uint32_t)
+BK_DEFINE_SORT_BATCH_K(i64, int64_t)
+BK_DEFINE_SORT_BATCH_K(u64, uint64_t)
+BK_DEFINE_SORT_BATCH_K(f32, float)
+BK_DEFINE_SORT_BATCH_K(f64, double)

@@ -278,6 +278,34 @@ BK_API int bk_reduce_by_key_i64_i64_batch(const bk_rbk_item_i64_i64 *items, uint
 BK_API int bk_reduce_by_key_i64_f32_batch(const bk_rbk_item_i64_f32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_reduce_by_key_i64_f64_batch(const bk_rbk_item_i64_f64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
+/* Stable sort_by_key of up to BK_BATCH_MAX arrays, each in place (as
+ * bk_sort_by_key_*): one block-sort launch for all arrays, then per merge
+ * pass one launch for all arrays that still need it. */
+typedef struct bk_sort_item_i32_u32 { int32_t *keys; uint32_t *vals; uint64_t n; } bk_sort_item_i32_u32;
+typedef struct bk_sort_item_i32_u64 { int32_t *keys; uint64_t *vals; uint64_t n; } bk_sort_item_i32_u64;
+typedef struct bk_sort_item_u32_u32 { uint32_t *keys; uint32_t *vals; uint64_t n; } bk_sort_item_u32_u32;
+typedef struct bk_sort_item_u32_u64 { uint32_t *keys; uint64_t *vals; uint64_t n; } bk_sort_item_u32_u64;
+typedef struct bk_sort_item_i64_u32 { int64_t *keys; uint32_t *vals; uint64_t n; } bk_sort_item_i64_u32;
+typedef struct bk_sort_item_i64_u64 { int64_t *keys; uint64_t *vals; uint64_t n; } bk_sort_item_i64_u64;
+typedef struct bk_sort_item_u64_u32 { uint64_t *keys; uint32_t *vals; uint64_t n; } bk_sort_item_u64_u32;
+typedef struct bk_sort_item_u64_u64 { uint64_t *keys; uint64_t *vals; uint64_t n; } bk_sort_item_u64_u64;
+typedef struct bk_sort_item_f32_u32 { float *keys; uint32_t *vals; uint64_t n; } bk_sort_item_f32_u32;
+typedef struct bk_sort_item_f32_u64 { float *keys; uint64_t *vals; uint64_t n; } bk_sort_item_f32_u64;
+typedef struct bk_sort_item_f64_u32 { double *keys; uint32_t *vals; uint64_t n; } bk_sort_item_f64_u32;
+typedef struct bk_sort_item_f64_u64 { double *keys; uint64_t *vals; uint64_t n; } bk_sort_item_f64_u64;
+BK_API int bk_sort_by_key_i32_u32_batch(const bk_sort_item_i32_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i32_u64_batch(const bk_sort_item_i32_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u32_u32_batch(const bk_sort_item_u32_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u32_u64_batch(const bk_sort_item_u32_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i64_u32_batch(const bk_sort_item_i64_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i64_u64_batch(const bk_sort_item_i64_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u64_u32_batch(const bk_sort_item_u64_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u64_u64_batch(const bk_sort_item_u64_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f32_u32_batch(const bk_sort_item_f32_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f32_u64_batch(const bk_sort_item_f32_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f64_u32_batch(const bk_sort_item_f64_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f64_u64_batch(const bk_sort_item_f64_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -18,7 +18,7 @@ import torch
 import bulk_b200
 import oracle
 from bulk_b200 import _lib
-from bulk_b200.batch import batch_workspace_bytes, rbk_item_type, scan_item_type
+from bulk_b200.batch import batch_workspace_bytes, rbk_item_type, scan_item_type, sort_item_type
 
 ROOT_HEADER = _lib.HEADER.read_text()
 TAGS = ["i32", "u32", "i64", "u64", "f32", "f64"]
@@ -36,6 +36,9 @@ def test_header_declares_batch_entry_points():
         assert re.search(rf"typedef struct bk_scan_item_{t} \{{", ROOT_HEADER)
     for k, v in RBK_COMBOS:
         assert f"bk_reduce_by_key_{k}_{v}_batch(" in ROOT_HEADER
+    for t in TAGS:
+        for v in ("u32", "u64"):
+            assert f"bk_sort_by_key_{t}_{v}_batch(" in ROOT_HEADER
     assert "#define BK_BATCH_MAX 256" in ROOT_HEADER and bulk_b200.BATCH_MAX == 256
 
 
@@ -48,6 +51,20 @@ def test_scan_item_layout(tag):
 @pytest.mark.parametrize("kv", RBK_COMBOS)
 def test_rbk_item_layout(kv):
     assert ctypes.sizeof(rbk_item_type(*kv)) == 48
+
+
+def test_sort_item_layout_and_workspace():
+    assert ctypes.sizeof(sort_item_type("u32", "u32")) == 24
+    # per array: key and payload temporaries and the pass splits (each 256-aligned);
+    # arrays of 0 or 1 elements need nothing
+    def one(n, ks, vs, tile):
+        r = lambda b: (b + 255) // 256 * 256
+        return r(n * ks) + r(n * vs) + r(((n + tile - 1) // tile + 1) * 8)
+    sizes = [0, 1, 2, 5000, 1 << 20]
+    want = 256 + sum(one(n, 4, 4, 4096) for n in sizes if n > 1)
+    assert batch_workspace_bytes("sort_by_key", "u32", "u32", sizes) == want
+    assert batch_workspace_bytes("sort_by_key", "u32", "u32", [1 << 20]) == bulk_b200.workspace_bytes(
+        "sort_by_key", "u32", "u32", 1 << 20)
 
 
 def test_batch_workspace_bytes_counts_every_arrays_tiles():
@@ -181,3 +198,29 @@ def test_reduce_by_key_batch_counts_stay_on_device(cuda):
     counts = [int(c.item()) for _, _, c in res]
     assert counts == [3, 0, 1]
     assert res[0][0][:3].tolist() == [1, 2, 3] and res[0][1][:3].tolist() == [1.0, 2.0, 12.0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kv", [("u32", "u32"), ("f32", "u32"), ("i64", "u32"), ("u64", "u64"), ("f64", "u64")])
+def test_sort_batch_matches_each_array_alone(cuda, kv):
+    """Stable order: payload = original index, ties (few distinct keys) must
+    keep it; sizes span 0..2^20 so the arrays need 0..7 merge passes."""
+    from tests.gpu_util import NP, dev, host
+    kt, vt = kv
+    sizes = [0, 1, 2, 100, 4095, 4096, 8193, 20000, 1 << 16, 300001, 1 << 20, 7]
+    keys_h, vals_h = [], []
+    for i, n in enumerate(sizes):
+        rng = np.random.default_rng(600 + i)
+        if kt in ("f32", "f64"):
+            k = rng.integers(0, 50, n).astype(NP[kt]) / 4
+        else:
+            k = rng.integers(0, 1000 if i % 2 else 1 << 30, n).astype(NP[kt])
+        keys_h.append(k)
+        vals_h.append(np.arange(n, dtype=NP[vt]))
+    dk = [dev(k) for k in keys_h]
+    dv = [dev(v) for v in vals_h]
+    bulk_b200.stable_sort_by_key_batch(dk, dv)
+    for k, v, gk, gv in zip(keys_h, vals_h, dk, dv):
+        order = np.argsort(k, kind="stable")
+        assert np.array_equal(host(gk), k[order]), f"n={k.size}"
+        assert np.array_equal(host(gv), v[order]), f"n={k.size}"
