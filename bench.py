@@ -17,6 +17,13 @@ ops    = per-op GB/s: the headline's six calls, and the other benchmark
          2^26 u32/u64 keys with u32 payload, reduce_by_key 2^27 i32 keys with
          geometric / Zipf runs and f32 / f64 values), timed after the headline.
 
+serving = plain vs batched serving of a mixed request stream (bulk_b200/serve.py:
+         40% sort_by_key u32/u32, 30% reduce_by_key i32/f32, 30% scan f32;
+         sizes log-uniform in [2^10, 2^24], and a small-request variant in
+         [2^10, 2^16]): saturation req/s and, at 2000 req/s Poisson arrivals,
+         p50/p99 latency, for one call per request ("plain") and continuous
+         batching ("batched"); rank 0 only.
+
 ``--impl reference`` times the reference's CPU implementation of the same
 reduce + scan on the host cores instead (rank 0 only).
 """
@@ -452,6 +459,7 @@ def main(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-other-ops", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--ops-shift", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
     if args.warmup < 3:
@@ -521,6 +529,12 @@ def main(argv=None):
             "gpu_launches": args.steps * 9,
             "clocks": clocks,
         }
+    if rank == 0 and not args.no_serving:
+        from bulk_b200 import serve
+        sv = serve.benchmark(saturation_requests=600, rate=2000.0, open_loop_s=1.0)
+        small = serve.benchmark(saturation_requests=2000, rate=2000.0, open_loop_s=1.0, hi=1 << 16)
+        line["serving"] = {"mix_2^10_2^24": sv, "mix_2^10_2^16": small}
+        torch.cuda.empty_cache()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

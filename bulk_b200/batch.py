@@ -88,13 +88,15 @@ def inclusive_scan_batch(xs, inits=None, outs=None, stream: torch.cuda.Stream | 
     return outs
 
 
-def reduce_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | None = None, sync: bool = False):
+def reduce_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | None = None, sync: bool = False,
+                        outs=None):
     """reduce_by_key (equal keys, sum) of every (keys, vals) pair.
 
     Returns a list of (out_keys, out_vals, count): with ``sync=False`` count
     is a 1-element device tensor and the outputs are full-length buffers; with
     ``sync=True`` (one synchronisation for the whole batch) counts are ints and
-    the outputs are trimmed."""
+    the outputs are trimmed.  ``outs`` optionally supplies the buffers: one
+    (out_keys, out_vals, count) per pair, count a 1-element int64 tensor."""
     keys_list, vals_list = list(keys_list), list(vals_list)
     if len(keys_list) != len(vals_list):
         raise ValueError("keys_list and vals_list must have the same length")
@@ -110,24 +112,33 @@ def reduce_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | None =
     s = _stream_handle(stream, dev)
     item_t = rbk_item_type(kt, vt)
     fn = getattr(lib, f"bk_reduce_by_key_{kt}_{vt}_batch")
-    counts = torch.empty(len(keys_list), dtype=torch.int64, device=dev)
-    res = []
-    for k, v in zip(keys_list, vals_list):
-        res.append((torch.empty(max(k.numel(), 1), dtype=k.dtype, device=dev),
-                    torch.empty(max(v.numel(), 1), dtype=v.dtype, device=dev)))
+    if outs is not None:
+        outs = list(outs)
+        if len(outs) != len(keys_list):
+            raise ValueError("one (out_keys, out_vals, count) per pair")
+        _require_cuda(*(t for o in outs for t in o))
+        res = [(o[0], o[1]) for o in outs]
+        cnt = [o[2] for o in outs]
+    else:
+        counts = torch.empty(len(keys_list), dtype=torch.int64, device=dev)
+        res = []
+        for k, v in zip(keys_list, vals_list):
+            res.append((torch.empty(max(k.numel(), 1), dtype=k.dtype, device=dev),
+                        torch.empty(max(v.numel(), 1), dtype=v.dtype, device=dev)))
+        cnt = [counts[i:i + 1] for i in range(len(keys_list))]
     for lo, hi in _chunks(len(keys_list)):
         items = (item_t * (hi - lo))()
         for j, i in enumerate(range(lo, hi)):
             it = items[j]
             it.keys, it.vals, it.n = keys_list[i].data_ptr(), vals_list[i].data_ptr(), keys_list[i].numel()
             it.out_keys, it.out_vals = res[i][0].data_ptr(), res[i][1].data_ptr()
-            it.d_num_out = counts[i:i + 1].data_ptr()
+            it.d_num_out = cnt[i].data_ptr()
         need = batch_workspace_bytes("reduce_by_key", kt, vt, [keys_list[i].numel() for i in range(lo, hi)])
         ws, wsb = workspaces.get(max(need, 256), dev, s)
         check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
     if not sync:
-        return [(ok, ov, counts[i:i + 1]) for i, (ok, ov) in enumerate(res)]
-    cs = counts.tolist()
+        return [(ok, ov, cnt[i]) for i, (ok, ov) in enumerate(res)]
+    cs = [int(c) for c in torch.cat([c.view(1) for c in cnt]).tolist()]
     return [(ok[:c], ov[:c], c) for (ok, ov), c in zip(res, cs)]
 
 
