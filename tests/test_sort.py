@@ -1,5 +1,7 @@
-"""GPU parity of bk_sort_by_key_* / bk_sort_keys_* (stable merge sort) against
-the oracle: keys and payload order bit-exact."""
+"""GPU parity of bk_sort_by_key_* / bk_sort_keys_* against the oracle: keys
+and payload order bit-exact.  Below 2^30 elements the library sorts by stable
+LSD radix, at and above it by merging; a stable sort's output is unique, so
+both must equal the oracle's stable merge sort."""
 from __future__ import annotations
 
 import numpy as np
@@ -98,3 +100,37 @@ def test_full_size_2_26_payload_is_index(cuda, tag):
     assert bool(ok.all())
     assert torch.equal(torch.sort(vals).values, torch.arange(n, dtype=torch.int32, device=cuda))
     assert torch.equal(ks, k0[vals.long()])
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_signed_zeros_infinities_and_denormals_keep_stable_order(cuda, tag):
+    """-0.0 and +0.0 compare equal, so they tie and keep their input order;
+    the keys come back with their own bit patterns."""
+    dt = NP[tag]
+    tiny = np.finfo(dt).smallest_subnormal
+    special = np.array([0.0, -0.0, np.inf, -np.inf, tiny, -tiny, 1.0, -1.0, np.finfo(dt).max, -np.finfo(dt).max],
+                       dtype=dt)
+    rng = np.random.default_rng(11)
+    for n in (10, 4097, 70001):
+        keys = special[rng.integers(0, special.size, n)]
+        vals = np.arange(n, dtype=np.uint32)
+        gk, gv = bulk_b200.stable_sort_by_key(dev(keys), dev(vals))
+        wk, wv = oracle.stable_sort_by_key(keys, vals)
+        ut = np.uint32 if tag == "f32" else np.uint64
+        assert np.array_equal(host(gk).view(ut), wk.view(ut)), n
+        assert np.array_equal(host(gv), wv), n
+
+
+@pytest.mark.slow
+def test_merge_path_at_2_30(cuda):
+    """2^30 elements, the first size sorted by merging: i32 keys with many
+    duplicates, payload = index, against torch's stable sort."""
+    n = 1 << 30
+    g = torch.Generator(device=cuda)
+    g.manual_seed(5)
+    keys = torch.randint(-(1 << 20), 1 << 20, (n,), generator=g, device=cuda, dtype=torch.int32)
+    want = torch.sort(keys, stable=True)
+    vals = torch.arange(n, dtype=torch.int32, device=cuda)
+    bulk_b200.stable_sort_by_key(keys, vals)
+    assert torch.equal(keys, want.values)
+    assert torch.equal(vals, want.indices.to(torch.int32))
