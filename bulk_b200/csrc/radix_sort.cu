@@ -19,10 +19,11 @@
 //              scan): in digit-major order the scanned value of (d, t) minus
 //              the count itself is exactly where tile t's keys of digit d
 //              start in the output;
-//   downsweep  each tile ranks its keys by digit (per-warp counters advanced
-//              with __match_any_sync, which keeps input order inside a
-//              digit), stages them in shared memory in digit order and writes
-//              each digit's run contiguously to its position.
+//   downsweep  each tile ranks its keys by digit (the lanes of a warp that
+//              share a digit are found with eight ballots; per-warp counters
+//              keep input order inside a digit), stages them in shared memory
+//              in digit order and writes each digit's run contiguously to its
+//              position.
 // A batch lays its arrays' count regions one after another, so the one scan
 // serves all of them: an array's positions are the scanned values minus the
 // number of elements of the arrays before it.
@@ -93,8 +94,8 @@ __device__ __forceinline__ int rs_digit(K k, int shift) {
 }
 
 // Lanes of the warp whose 8-bit digit equals this lane's, from eight
-// ballots.  __match_any_sync gives the same mask but runs on a slow shared
-// unit; eight votes keep the ranking off it.
+// ballots (__match_any_sync gives the same mask, but on a unit that
+// saturated at one match a key here).
 __device__ __forceinline__ unsigned int rs_peers(unsigned int d) {
   unsigned int peers = 0xffffffffu;
 #pragma unroll
@@ -159,18 +160,21 @@ struct RsBatch {
 };
 
 // Upsweep: the tile's count of every digit, stored digit-major.  Keys are
-// read warp-striped (element w*512 + j*32 + lane: coalesced).
+// read warp-striped (element w*512 + j*32 + lane: coalesced) and counted with
+// shared-memory atomics into one histogram per warp; a warp whose 32 keys
+// share one digit adds 32 with one atomic (constant high digits are common).
 template <typename K, typename P, typename Src>
 __global__ void __launch_bounds__(kRsThreads) rs_upsweep_kernel(const __grid_constant__ Src src, int pass,
                                                                 unsigned int *counts) {
-  __shared__ unsigned int s_cnt[kRsBins];
+  __shared__ unsigned int s_wcnt[kRsWarps][kRsBins];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int shift = 8 * pass;
   const RsTile<K, P> tl = src.tile(blockIdx.x);
   const K *in_k = (pass & 1) ? tl.tk : tl.keys;
   const uint64_t tbase = (uint64_t)tl.local * kRsTile;
   const int count = (int)((tl.n - tbase) < (uint64_t)kRsTile ? (tl.n - tbase) : (uint64_t)kRsTile);
-  s_cnt[tid] = 0u;
+#pragma unroll
+  for (int w = 0; w < kRsWarps; ++w) s_wcnt[w][tid] = 0u;
   __syncthreads();
   K k[kRsItems];
 #pragma unroll
@@ -180,16 +184,19 @@ __global__ void __launch_bounds__(kRsThreads) rs_upsweep_kernel(const __grid_con
   }
 #pragma unroll
   for (int j = 0; j < kRsItems; ++j) {
-    const int e = warp * 32 * kRsItems + j * 32 + lane;
-    // one shared-memory atomic per distinct digit among the warp's 32 keys;
-    // past the tile's end the digit is 255 and taken off below
-    const unsigned int d = e < count ? (unsigned int)rs_digit(k[j], shift) : kRsBins - 1u;
-    const unsigned int peers = rs_peers(d);
-    if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[d], (unsigned int)__popc(peers));
+    const bool valid = warp * 32 * kRsItems + j * 32 + lane < count;
+    const unsigned int d = (unsigned int)rs_digit(k[j], shift);
+    const unsigned int d0 = __shfl_sync(0xffffffffu, d, 0);
+    if (__all_sync(0xffffffffu, valid && d == d0)) {
+      if (lane == 0) atomicAdd(&s_wcnt[warp][d0], 32u);
+    } else if (valid) {
+      atomicAdd(&s_wcnt[warp][d], 1u);
+    }
   }
   __syncthreads();
-  unsigned int c = s_cnt[tid];
-  if (tid == kRsBins - 1) c -= (unsigned int)(kRsTile - count);
+  unsigned int c = 0;
+#pragma unroll
+  for (int w = 0; w < kRsWarps; ++w) c += s_wcnt[w][tid];
   counts[tl.count_base + (uint64_t)tid * tl.tiles + tl.local] = c;
 }
 
@@ -197,17 +204,23 @@ __global__ void __launch_bounds__(kRsThreads) rs_upsweep_kernel(const __grid_con
 // back on odd ones) to the positions the scan gave.  If the count scan
 // reported an error its positions are not trusted: the pass writes nothing
 // and the error is copied into the sort's own workspace header.
-template <typename K, typename P, typename Src>
-__global__ void __launch_bounds__(kRsThreads, sizeof(K) + payload_bytes<P>() == 4 ? 3 : 2) rs_downsweep_kernel(
+template <int TH, typename K, typename P>
+constexpr int rs_down_min_blocks() {
+  return TH == 512 ? 2 : (sizeof(K) == 4 && payload_bytes<P>() <= 4 ? 3 : 2);
+}
+// TH threads; V = 1 finds every item's peers before the ranking chain
+// (more registers, more independent ballots), V = 0 item by item.
+template <typename K, typename P, typename Src, int V, int TH>
+__global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downsweep_kernel(
     const __grid_constant__ Src src, int pass, const unsigned int *scanned, const WsHeader *scan_hdr,
     WsHeader *hdr) {
+  constexpr int ITEMS = kRsTile / TH, WARPS = TH / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   K *sk = reinterpret_cast<K *>(smem);  // the tile in digit order
   P *sv = reinterpret_cast<P *>(smem + align_up(sizeof(K) * kRsTile, 16));
-  __shared__ unsigned int s_whist[kRsWarps][kRsBins];  // per-warp digit counters
-  __shared__ unsigned int s_tile_excl[kRsBins];
+  __shared__ unsigned int s_whist[WARPS][kRsBins];  // per-warp digit counters
   __shared__ unsigned int s_dst[kRsBins];  // output position of tile position 0 for digit d (mod 2^32)
-  __shared__ unsigned int s_scan[kRsBins / 32 + 1];
+  __shared__ unsigned int s_scan[TH / 32 + 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int scan_status = scan_hdr->status;
   if (scan_status != 0) {
@@ -222,69 +235,85 @@ __global__ void __launch_bounds__(kRsThreads, sizeof(K) + payload_bytes<P>() == 
   P *out_v = (pass & 1) ? tl.vals : tl.tv;
   const uint64_t tbase = (uint64_t)tl.local * kRsTile;
   const int count = (int)((tl.n - tbase) < (uint64_t)kRsTile ? (tl.n - tbase) : (uint64_t)kRsTile);
-  for (int i = tid; i < kRsWarps * kRsBins; i += kRsThreads) (&s_whist[0][0])[i] = 0u;
+  for (int i = tid; i < WARPS * kRsBins; i += TH) (&s_whist[0][0])[i] = 0u;
   __syncthreads();
 
-  K k[kRsItems];
-  P v[kRsItems];
-  auto elem = [&](int j) { return warp * 32 * kRsItems + j * 32 + lane; };
+  K k[ITEMS];
+  P v[ITEMS];
+  auto elem = [&](int j) { return warp * 32 * ITEMS + j * 32 + lane; };
   // digit of item j, recomputed where needed.  Past the tile's end it is
   // 255: those items come after every real one in (warp, item, lane) order,
   // so they rank last in the tile and are never written out.
   auto digit_of = [&](int j) { return elem(j) < count ? rs_digit(k[j], shift) : kRsBins - 1; };
 #pragma unroll
-  for (int j = 0; j < kRsItems; ++j) {
+  for (int j = 0; j < ITEMS; ++j) {
     const bool ok = elem(j) < count;
     k[j] = ok ? in_k[tbase + elem(j)] : K();
     if constexpr (has_payload<P>()) v[j] = ok ? in_v[tbase + elem(j)] : P();
   }
   // rank within the warp: keys of one digit in input order (a rank is below
-  // 512, so two share a register)
-  unsigned int rank2[kRsItems / 2];
+  // 512, so two share a register).  The lowest lane of each digit reserves
+  // the digit's keys in the warp's counter; the shuffle that hands the old
+  // count to the other lanes also orders item j's atomic before item j+1's.
+  unsigned int rank2[ITEMS / 2];
   const unsigned int lt = (1u << lane) - 1u;
+  unsigned int pm[V == 1 ? ITEMS : 1];
+  if constexpr (V == 1) {
 #pragma unroll
-  for (int j = 0; j < kRsItems; ++j) {
+    for (int j = 0; j < ITEMS; ++j) pm[j] = rs_peers((unsigned int)digit_of(j));
+  }
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
     const int dj = digit_of(j);
-    const unsigned int peers = rs_peers((unsigned int)dj);
-    const unsigned int before = s_whist[warp][dj];
+    unsigned int peers;
+    if constexpr (V == 1) peers = pm[j];
+    else peers = rs_peers((unsigned int)dj);
+    const int leader = __ffs(peers) - 1;
+    unsigned int before = 0;
+    if (lane == leader) before = atomicAdd(&s_whist[warp][dj], (unsigned int)__popc(peers));
+    before = __shfl_sync(0xffffffffu, before, leader);
     const unsigned int r = before + __popc(peers & lt);
     if (j & 1) rank2[j >> 1] |= r << 16;
     else rank2[j >> 1] = r;
-    __syncwarp();
-    if (lane == 31 - __clz(peers)) s_whist[warp][dj] = before + __popc(peers);
-    __syncwarp();
   }
   __syncthreads();
 
-  // thread d: the digit's offset in each warp and its tile count
+  // thread d < 256: the digit's tile count, then its start in the staged
+  // tile for each warp (the tile's exclusive count plus the warps before)
   const int d = tid;
   unsigned int cnt = 0;
+  if (d < kRsBins) {
 #pragma unroll
-  for (int w = 0; w < kRsWarps; ++w) {
-    const unsigned int c = s_whist[w][d];
-    s_whist[w][d] = cnt;
-    cnt += c;
+    for (int w = 0; w < WARPS; ++w) cnt += s_whist[w][d];
   }
   unsigned int tile_total;
-  const unsigned int tile_excl = block_exclusive_scan<kRsThreads>(cnt, OpSum<unsigned int>(), s_scan, tile_total);
-  if (d == kRsBins - 1) cnt -= (unsigned int)(kRsTile - count);  // real keys of digit 255
-  const unsigned int incl = scanned[tl.count_base + (uint64_t)d * tl.tiles + tl.local];
-  s_tile_excl[d] = tile_excl;
-  s_dst[d] = incl - cnt - tl.elem_base - tile_excl;
+  const unsigned int tile_excl = block_exclusive_scan<TH>(cnt, OpSum<unsigned int>(), s_scan, tile_total);
+  if (d < kRsBins) {
+    unsigned int run = tile_excl;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+      const unsigned int c = s_whist[w][d];
+      s_whist[w][d] = run;
+      run += c;
+    }
+    if (d == kRsBins - 1) cnt -= (unsigned int)(kRsTile - count);  // real keys of digit 255
+    const unsigned int incl = scanned[tl.count_base + (uint64_t)d * tl.tiles + tl.local];
+    s_dst[d] = incl - cnt - tl.elem_base - tile_excl;
+  }
   __syncthreads();
 
   // stage in digit order
 #pragma unroll
-  for (int j = 0; j < kRsItems; ++j) {
+  for (int j = 0; j < ITEMS; ++j) {
     const int dj = digit_of(j);
     const unsigned int rank = (rank2[j >> 1] >> (16 * (j & 1))) & 0xffffu;
-    const unsigned int pos = s_tile_excl[dj] + s_whist[warp][dj] + rank;
+    const unsigned int pos = s_whist[warp][dj] + rank;
     sk[pos] = k[j];
     if constexpr (has_payload<P>()) sv[pos] = v[j];
   }
   __syncthreads();
   // write out: position p of the staged tile goes to s_dst[digit] + p
-  for (int p = tid; p < count; p += kRsThreads) {
+  for (int p = tid; p < count; p += TH) {
     const K key = sk[p];
     const uint64_t g = (uint64_t)(s_dst[rs_digit(key, shift)] + (unsigned int)p);
     if (g < tl.n) {  // always true when the counts are consistent
@@ -339,6 +368,11 @@ size_t radix_sort_batch_ws_bytes(const uint64_t *sizes, uint32_t count) {
 // The passes over `src` (one array or a batch): upsweep, scan, downsweep each.
 template <typename K, typename P, typename Src>
 int radix_sort_run(const Src &src, const RsLayout<K, P> &L, char *ws, cudaStream_t stream) {
+  // measured on 2^26 keys with a 4-byte payload: 256 threads ranking item
+  // by item for 4-byte keys, 512 threads with every item's peers found
+  // first for 8-byte keys
+  constexpr int kDownTh = sizeof(K) == 8 ? 512 : 256;
+  constexpr int kDownV = sizeof(K) == 8 ? 1 : 0;
   int st;
   auto *counts = reinterpret_cast<unsigned int *>(ws + L.counts);
   void *scan_ws = ws + L.scan_ws;
@@ -346,7 +380,8 @@ int radix_sort_run(const Src &src, const RsLayout<K, P> &L, char *ws, cudaStream
   const auto *scan_hdr = reinterpret_cast<const WsHeader *>(scan_ws);
   static thread_local bool attr_set = false;
   if (!attr_set) {
-    if ((st = host::set_smem_attrs(rs_downsweep_kernel<K, P, Src>, rs_smem_bytes<K, P>())) != BK_OK) return st;
+    if ((st = host::set_smem_attrs(rs_downsweep_kernel<K, P, Src, kDownV, kDownTh>, rs_smem_bytes<K, P>())) != BK_OK)
+      return st;
     attr_set = true;
   }
   // the scan's workspace must start zeroed, like any workspace
@@ -357,7 +392,7 @@ int radix_sort_run(const Src &src, const RsLayout<K, P> &L, char *ws, cudaStream
     st = bk_inclusive_scan_sum_u32(counts, L.tiles * kRsBins, 0u, counts, scan_ws, L.scan_ws_bytes,
                                    (bk_stream_t)stream);
     if (st != BK_OK) return st;
-    rs_downsweep_kernel<K, P, Src><<<(unsigned)L.tiles, kRsThreads, rs_smem_bytes<K, P>(), stream>>>(
+    rs_downsweep_kernel<K, P, Src, kDownV, kDownTh><<<(unsigned)L.tiles, kDownTh, rs_smem_bytes<K, P>(), stream>>>(
         src, p, counts, scan_hdr, hdr);
     if ((st = host::launch_status()) != BK_OK) return st;
   }
