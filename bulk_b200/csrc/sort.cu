@@ -304,10 +304,17 @@ size_t merge_sort_ws_bytes_t(uint64_t n) {
          align_up((mp_tiles + 1) * sizeof(uint64_t), 256);
 }
 
-// Single-array sorts use the radix sort below 2^30 elements, the merge sort above.
+// Which sort an array gets: one block-sort launch when it fits one block
+// tile (the radix sort's passes are 4 or 8 times three launches), the radix
+// sort up to 2^30 elements, the merge sort above.
+template <typename K>
+bool use_radix(uint64_t n) {
+  return n > (uint64_t)SortCfg<K>::BS_TILE && n < kRadixMaxN;
+}
+
 template <typename K, typename P>
 size_t sort_ws_bytes_t(uint64_t n) {
-  return n < kRadixMaxN ? radix_sort_ws_bytes<K, P>(n) : merge_sort_ws_bytes_t<K, P>(n);
+  return use_radix<K>(n) ? radix_sort_ws_bytes<K, P>(n) : merge_sort_ws_bytes_t<K, P>(n);
 }
 
 template <typename Kern>
@@ -353,7 +360,7 @@ int sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaS
   if (st != BK_OK) return st;
   if (n <= 1) return BK_OK;
   if ((st = sort_check_array(keys, vals, n)) != BK_OK) return st;
-  if (n < kRadixMaxN) return radix_sort_launch<K, P>(keys, vals, n, d_ws, ws_bytes, stream);
+  if (use_radix<K>(n)) return radix_sort_launch<K, P>(keys, vals, n, d_ws, ws_bytes, stream);
   const uint64_t bs_tiles = (n + C::BS_TILE - 1) / C::BS_TILE;
   const uint64_t mp_tiles = (n + C::MP_TILE - 1) / C::MP_TILE;
   st = host::check_ws(d_ws, ws_bytes, sort_ws_bytes_t<K, P>(n));
@@ -409,12 +416,17 @@ size_t merge_sort_batch_ws_bytes_t(const uint64_t *sizes, uint32_t count) {
   return b;
 }
 
-// Batches whose arrays are all below 2^30 elements use the radix sort.
+// A batch uses the radix sort when all its arrays are below 2^30 elements
+// and one needs more than a block tile; otherwise the merge sort (a single
+// block-sort launch when every array fits one tile).
 template <typename K, typename P>
 bool sort_batch_radix(const uint64_t *sizes, uint32_t count) {
-  for (uint32_t i = 0; i < count; ++i)
+  bool any_large = false;
+  for (uint32_t i = 0; i < count; ++i) {
     if (sizes[i] >= kRadixMaxN) return false;
-  return true;
+    any_large = any_large || use_radix<K>(sizes[i]);
+  }
+  return any_large;
 }
 
 template <typename K, typename P>
@@ -429,10 +441,10 @@ int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, s
   if (count > 0 && items == nullptr) return BK_ERR_INVALID_ARGUMENT;
   if (count > (uint32_t)kSortBatchMax) return BK_ERR_TOO_LARGE;
   {
-    bool radix = true;
-    for (uint32_t i = 0; i < count; ++i) radix = radix && items[i].n < kRadixMaxN;
+    uint64_t sizes[kSortBatchMax];
+    for (uint32_t i = 0; i < count; ++i) sizes[i] = items[i].n;
     static_assert(sizeof(SortItem<K, P>) == sizeof(RsItem<K, P>), "same item layout");
-    if (radix)
+    if (sort_batch_radix<K, P>(sizes, count))
       return radix_sort_batch_launch<K, P>(reinterpret_cast<const RsItem<K, P> *>(items), count, d_ws, ws_bytes,
                                            stream);
   }

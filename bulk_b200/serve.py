@@ -12,77 +12,74 @@ request is one of
 
 of n elements, n log-uniform in [lo, hi].  Arrivals are Poisson.  Inputs are
 synthetic and seeded: a request's input is a window (chosen by its id) of a
-pre-generated source array of its kind, so it depends only on the id.  Scan
-and reduce_by_key read their window in place; a sort copies its keys and
-payload into its own buffers.  Outputs and sort buffers come from a pooled
-device allocator; admission keeps the bytes of admitted, unfinished requests
-within an HBM budget.
+pre-generated source array of its kind, so it depends only on the id.
 
-``plain`` issues every admitted request as its own call (bk_* single-array
-entry points) on one stream, in arrival order.  ``batched`` gathers all
-admitted requests that have arrived, groups them by kind and issues one
-batched call per kind (bk_*_batch), keeping at most ``max_inflight`` batches
-queued on the stream; a request completes when its call's event does.
-Latency = completion time - arrival time, on the host's clock.
+The loop itself is native (``bk_serve_run`` in libbulkb200.so): admission in
+arrival order against an HBM budget, a pooled first-fit allocator over one
+device buffer, issue on one stream, completion by event polling.  ``plain``
+issues every admitted request as its own call (the single-array entry
+points); ``batched`` issues every admitted request that has arrived at once,
+one batched call per kind, with at most ``max_inflight`` batches queued.
+Latency = completion time - arrival time, on the host's steady clock.  This
+module builds the request stream and the sources, and reads the records.
 """
 from __future__ import annotations
 
-import bisect
+import ctypes
 import math
-import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 import torch
 
-from . import algorithms, batch
-from .algorithms import inclusive_scan, reduce_by_key, stable_sort_by_key
+from . import _lib
+from ._lib import check, lib
+from .algorithms import _require_cuda, _stream_handle
 
 KINDS = ("sort", "rbk", "scan")
 
 
 # --------------------------------------------------------------------------
 class DevicePool:
-    """Pooled allocator over one preallocated byte buffer: first-fit over an
+    """The serving loop's pooled allocator (bk_pool_*: first fit over an
     address-ordered free list, 256-byte granules, neighbours coalesced on
-    free.  Allocation never calls into the CUDA allocator."""
+    free) over a byte buffer of ``capacity`` bytes on ``device``."""
 
     ALIGN = 256
 
     def __init__(self, capacity: int, device="cuda"):
         self.capacity = capacity // self.ALIGN * self.ALIGN
         self.buf = torch.empty(self.capacity, dtype=torch.uint8, device=device)
-        self._free = [(0, self.capacity)]  # (offset, size), sorted by offset
-        self._used: dict[int, int] = {}
-        self.in_use = 0
-        self.high_water = 0
+        self._h = lib.bk_pool_create(self.capacity)
+        if not self._h:
+            raise MemoryError("bk_pool_create failed")
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            lib.bk_pool_destroy(h)
 
     def alloc(self, nbytes: int) -> int | None:
-        need = max(self.ALIGN, -(-nbytes // self.ALIGN) * self.ALIGN)
-        for i, (off, size) in enumerate(self._free):
-            if size >= need:
-                if size == need:
-                    del self._free[i]
-                else:
-                    self._free[i] = (off + need, size - need)
-                self._used[off] = need
-                self.in_use += need
-                self.high_water = max(self.high_water, self.in_use)
-                return off
-        return None
+        off = ctypes.c_uint64()
+        st = lib.bk_pool_alloc(self._h, nbytes, ctypes.byref(off))
+        if st == _lib.BK_ERR_TOO_LARGE:
+            return None
+        check(st, "bk_pool_alloc")
+        return off.value
 
     def free(self, off: int) -> None:
-        size = self._used.pop(off)
-        self.in_use -= size
-        i = bisect.bisect_left(self._free, (off, 0))
-        self._free.insert(i, (off, size))
-        # coalesce with the right, then the left neighbour
-        if i + 1 < len(self._free) and off + size == self._free[i + 1][0]:
-            self._free[i] = (off, size + self._free[i + 1][1])
-            del self._free[i + 1]
-        if i > 0 and self._free[i - 1][0] + self._free[i - 1][1] == off:
-            self._free[i - 1] = (self._free[i - 1][0], self._free[i - 1][1] + self._free[i][1])
-            del self._free[i]
+        check(lib.bk_pool_free(self._h, off), "bk_pool_free")
+
+    @property
+    def in_use(self) -> int:
+        return lib.bk_pool_in_use(self._h)
+
+    @property
+    def high_water(self) -> int:
+        return lib.bk_pool_high_water(self._h)
+
+    def free_blocks(self) -> int:
+        return lib.bk_pool_free_blocks(self._h)
 
     def view(self, off: int, n: int, dtype: torch.dtype) -> torch.Tensor:
         nbytes = n * torch.empty(0, dtype=dtype).element_size()
@@ -96,16 +93,12 @@ class Request:
     kind: str
     n: int
     arrival: float  # seconds from the start of the run
-    allocs: list = field(default_factory=list)
-    tensors: dict = field(default_factory=dict)
     start: float = math.nan
     done: float = math.nan
-    event: torch.cuda.Event | None = None
 
     def nbytes(self) -> int:
-        # the request's own buffers (sort: keys and payload; rbk: outputs and
-        # the count word; scan: output); workspaces are shared per stream
-        return {"sort": 8, "rbk": 8, "scan": 4}[self.kind] * self.n + 512
+        """Bytes the request holds while admitted (its own buffers)."""
+        return lib.bk_serve_request_bytes(KINDS.index(self.kind), self.n)
 
 
 def make_requests(count: int, rate: float, seed: int = 1000, lo: int = 1 << 10, hi: int = 1 << 24,
@@ -142,145 +135,90 @@ class Sources:
         return (req.rid * 2654435761) % span // 64 * 64
 
 
+class _Request(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("n", ctypes.c_uint64),
+                ("src_offset", ctypes.c_uint64), ("arrival_s", ctypes.c_double)]
+
+
+class _Record(ctypes.Structure):
+    _fields_ = [("start_s", ctypes.c_double), ("done_s", ctypes.c_double), ("out", ctypes.c_uint64 * 3)]
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("sort_keys", ctypes.c_void_p), ("sort_vals", ctypes.c_void_p), ("rbk_keys", ctypes.c_void_p),
+                ("rbk_vals", ctypes.c_void_p), ("scan_vals", ctypes.c_void_p), ("source_len", ctypes.c_uint64),
+                ("pool", ctypes.c_void_p), ("pool_bytes", ctypes.c_uint64), ("ws", ctypes.c_void_p),
+                ("ws_bytes", ctypes.c_uint64), ("budget_bytes", ctypes.c_uint64), ("stream", ctypes.c_void_p),
+                ("mode", ctypes.c_int32), ("max_inflight", ctypes.c_int32), ("keep_buffers", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("timeout_s", ctypes.c_double)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("makespan_s", ctypes.c_double), ("pool_high_water", ctypes.c_uint64), ("calls", ctypes.c_uint64),
+                ("batches", ctypes.c_uint64)]
+
+
+MODES = {"plain": 0, "batched": 1}
+
+
 class Server:
+    """Runs request streams through bk_serve_run over `sources`, with the
+    requests' buffers in `pool`'s device buffer and at most `budget_bytes`
+    of them admitted at once."""
+
     def __init__(self, sources: Sources, pool: DevicePool, budget_bytes: int, stream=None, keep_results=False):
         self.src = sources
         self.pool = pool
         self.budget = budget_bytes
-        self.admitted_bytes = 0
-        self.stream = stream or torch.cuda.Stream()
+        dev = _require_cuda(sources.sort_keys)
+        self.stream = stream or torch.cuda.Stream(dev)
         self.keep = keep_results
         self.results: dict[int, tuple] = {}
+        self._ws = None
 
-    # ---- memory
-    def _admit(self, req: Request) -> bool:
-        # over budget: wait -- unless nothing is admitted (a request larger
-        # than the whole budget still runs, alone)
-        if self.admitted_bytes > 0 and self.admitted_bytes + req.nbytes() > self.budget:
-            return False
-        # the request's own buffers: slot -> (dtype, elements)
-        sizes = {"sort": {0: (torch.uint32, req.n), 1: (torch.uint32, req.n)},
-                 "rbk": {2: (torch.int32, req.n), 3: (torch.float32, req.n), 4: (torch.int64, 1)},
-                 "scan": {1: (torch.float32, req.n)}}[req.kind]
-        offs, tensors = [], {}
-        for slot, (dt, n) in sizes.items():
-            off = self.pool.alloc(n * torch.empty(0, dtype=dt).element_size())
-            if off is None:
-                for o in offs:
-                    self.pool.free(o)
-                return False
-            offs.append(off)
-            tensors[slot] = self.pool.view(off, n, dt)
-        # inputs read in place: windows of the sources
-        o, n = self.src.offset(req), req.n
-        if req.kind == "rbk":
-            tensors[0], tensors[1] = self.src.rbk_keys[o:o + n], self.src.rbk_vals[o:o + n]
-        elif req.kind == "scan":
-            tensors[0] = self.src.scan_vals[o:o + n]
-        req.allocs, req.tensors = offs, tensors
-        self.admitted_bytes += req.nbytes()
-        return True
+    def _workspace(self, reqs_arr, count: int, mode: int):
+        need = max(256, lib.bk_serve_workspace_bytes(ctypes.cast(reqs_arr, ctypes.c_void_p), count, mode))
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = torch.zeros(need, dtype=torch.uint8, device=self.pool.buf.device)
+        return self._ws
 
-    def _release(self, req: Request) -> None:
-        if self.keep:
-            t = req.tensors
-            if req.kind == "sort":
-                self.results[req.rid] = (t[0].clone(), t[1].clone())
-            elif req.kind == "rbk":
-                self.results[req.rid] = (t[2].clone(), t[3].clone(), t[4].clone())
-            else:
-                self.results[req.rid] = (t[1].clone(),)
-        for o in req.allocs:
-            self.pool.free(o)
-        req.allocs, req.tensors = [], {}
-        self.admitted_bytes -= req.nbytes()
-
-    def _stage(self, req: Request) -> None:
-        """A sort copies its input window into its own buffers (on the stream)."""
-        if req.kind == "sort":
-            o, n, t = self.src.offset(req), req.n, req.tensors
-            t[0].copy_(self.src.sort_keys[o:o + n], non_blocking=True)
-            t[1].copy_(self.src.sort_vals[o:o + n], non_blocking=True)
-
-    # ---- issue
-    def _issue_one(self, req: Request) -> None:
-        t = req.tensors
-        if req.kind == "sort":
-            stable_sort_by_key(t[0], t[1], stream=self.stream)
-        elif req.kind == "rbk":
-            reduce_by_key(t[0], t[1], t[2], t[3], t[4], stream=self.stream, sync=False)
-        else:
-            inclusive_scan(t[0], 0.0, out=t[1], stream=self.stream)
-
-    def _issue_batch(self, kind: str, reqs: list[Request]) -> None:
-        ts = [r.tensors for r in reqs]
-        if kind == "sort":
-            batch.stable_sort_by_key_batch([t[0] for t in ts], [t[1] for t in ts], stream=self.stream)
-        elif kind == "rbk":
-            batch.reduce_by_key_batch([t[0] for t in ts], [t[1] for t in ts], stream=self.stream,
-                                      outs=[(t[2], t[3], t[4]) for t in ts])
-        else:
-            batch.inclusive_scan_batch([t[0] for t in ts], [0.0] * len(ts), [t[1] for t in ts], stream=self.stream)
-
-    # ---- run
     def run(self, requests: list[Request], mode: str, max_inflight: int = 2, timeout_s: float = 120.0) -> dict:
         """Serve `requests` (sorted by arrival) in `mode` ("plain" or "batched")."""
         pending = sorted(requests, key=lambda r: r.arrival)
-        nxt = 0            # next request not yet admitted
-        waiting: list[Request] = []   # arrived and admitted, not issued (batched mode)
-        inflight: list[tuple[torch.cuda.Event, list[Request]]] = []
-        done = 0
-        t0 = time.perf_counter()
-        with torch.cuda.stream(self.stream):
-            while done < len(pending):
-                now = time.perf_counter() - t0
-                if now > timeout_s:
-                    raise TimeoutError(f"serving run exceeded {timeout_s} s")
-                # completions (in stream order)
-                while inflight and inflight[0][0].query():
-                    ev, reqs = inflight.pop(0)
-                    tdone = time.perf_counter() - t0
-                    for r in reqs:
-                        r.done = tdone
-                        self._release(r)
-                        done += 1
-                # arrivals and admission, in arrival order
-                now = time.perf_counter() - t0
-                while nxt < len(pending) and pending[nxt].arrival <= now and self._admit(pending[nxt]):
-                    r = pending[nxt]
-                    nxt += 1
-                    if mode == "plain":
-                        r.start = now
-                        self._stage(r)
-                        self._issue_one(r)
-                        ev = torch.cuda.Event()
-                        ev.record(self.stream)
-                        inflight.append((ev, [r]))
-                    else:
-                        waiting.append(r)
-                if mode == "batched" and waiting and len(inflight) < max_inflight:
-                    by_kind: dict[str, list[Request]] = {}
-                    for r in waiting:
-                        by_kind.setdefault(r.kind, []).append(r)
-                    issued = []
-                    for kind, reqs in by_kind.items():
-                        for lo in range(0, len(reqs), batch.BATCH_MAX):
-                            chunk = reqs[lo:lo + batch.BATCH_MAX]
-                            for r in chunk:
-                                r.start = now
-                                self._stage(r)
-                            self._issue_batch(kind, chunk)
-                            issued.extend(chunk)
-                    ev = torch.cuda.Event()
-                    ev.record(self.stream)
-                    inflight.append((ev, issued))
-                    waiting = []
-        makespan = time.perf_counter() - t0
-        lat = np.array([r.done - r.arrival for r in pending])
-        return {"mode": mode, "requests": len(pending), "makespan_s": makespan,
-                "req_per_s": len(pending) / makespan if makespan > 0 else math.inf,
+        count = len(pending)
+        arr = (_Request * max(count, 1))()
+        for i, r in enumerate(pending):
+            arr[i].kind, arr[i].n = KINDS.index(r.kind), r.n
+            arr[i].src_offset, arr[i].arrival_s = self.src.offset(r), r.arrival
+        recs = (_Record * max(count, 1))()
+        ws = self._workspace(arr, count, MODES[mode])
+        s = self.src
+        cfg = _Config(s.sort_keys.data_ptr(), s.sort_vals.data_ptr(), s.rbk_keys.data_ptr(), s.rbk_vals.data_ptr(),
+                      s.scan_vals.data_ptr(), s.n_max, self.pool.buf.data_ptr(), self.pool.capacity,
+                      ws.data_ptr(), ws.numel(), self.budget, _stream_handle(self.stream, self.pool.buf.device),
+                      MODES[mode], max_inflight, 1 if self.keep else 0, 0, timeout_s)
+        stats = _Stats()
+        torch.cuda.current_stream(self.pool.buf.device).synchronize()  # sources and buffers are ready
+        check(lib.bk_serve_run(ctypes.byref(cfg), ctypes.cast(arr, ctypes.c_void_p), count,
+                               ctypes.cast(recs, ctypes.c_void_p), ctypes.byref(stats)), "bk_serve_run")
+        for i, r in enumerate(pending):
+            r.start, r.done = recs[i].start_s, recs[i].done_s
+            if self.keep:
+                self.results[r.rid] = self._result(r, recs[i].out)
+        lat = np.array([r.done - r.arrival for r in pending]) if count else np.zeros(1)
+        return {"mode": mode, "requests": count, "makespan_s": stats.makespan_s,
+                "req_per_s": count / stats.makespan_s if stats.makespan_s > 0 else math.inf,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                "pool_high_water_bytes": self.pool.high_water}
+                "pool_high_water_bytes": stats.pool_high_water, "calls": stats.calls, "batches": stats.batches}
+
+    def _result(self, r: Request, out) -> tuple:
+        v = self.pool.view
+        if r.kind == "sort":
+            return v(out[0], r.n, torch.uint32).clone(), v(out[1], r.n, torch.uint32).clone()
+        if r.kind == "rbk":
+            return (v(out[0], r.n, torch.int32).clone(), v(out[1], r.n, torch.float32).clone(),
+                    v(out[2], 1, torch.int64).clone())
+        return (v(out[0], r.n, torch.float32).clone(),)
 
 
 def benchmark(saturation_requests: int = 600, rate: float = 2000.0, open_loop_s: float = 1.0, seed: int = 1000,
@@ -306,6 +244,7 @@ def benchmark(saturation_requests: int = 600, rate: float = 2000.0, open_loop_s:
         torch.cuda.synchronize()
         out[mode] = {"saturation_req_s": sat["req_per_s"], "saturation_p99_ms": sat["p99_ms"],
                      "open_loop_p50_ms": ol["p50_ms"], "open_loop_p99_ms": ol["p99_ms"],
-                     "open_loop_req_s": ol["req_per_s"]}
+                     "open_loop_req_s": ol["req_per_s"], "saturation_calls": sat["calls"],
+                     "saturation_batches": sat["batches"]}
     out["batched_over_plain_req_s"] = out["batched"]["saturation_req_s"] / out["plain"]["saturation_req_s"]
     return out

@@ -306,6 +306,87 @@ BK_API int bk_sort_by_key_f32_u64_batch(const bk_sort_item_f32_u64 *items, uint3
 BK_API int bk_sort_by_key_f64_u32_batch(const bk_sort_item_f64_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_sort_by_key_f64_u64_batch(const bk_sort_item_f64_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
+/* ---- serving loop -----------------------------------------------------------
+ * No counterpart in the reference, whose drivers run one array at a time.
+ * bk_serve_run answers a stream of mixed requests on one stream, either one
+ * library call per request (BK_SERVE_PLAIN: the single-array entry points
+ * above, sort inputs copied with cudaMemcpyAsync) or by continuous batching
+ * (BK_SERVE_BATCHED: every admitted request that has arrived is issued at
+ * once, one *_batch call per kind, sort inputs gathered by one copy kernel;
+ * at most max_inflight batches are queued on the stream).  A request reads
+ * a window of the caller's source arrays; its own buffers (sort: keys and
+ * payload, sorted in place; rbk: out_keys, out_vals, count; scan: output)
+ * come from a first-fit pool over the caller's device buffer, and requests
+ * are admitted in arrival order while the bytes of admitted, unfinished
+ * requests (bk_serve_request_bytes each) stay within budget_bytes; a request
+ * larger than the budget runs alone.  Start and done times are the host's
+ * steady clock, in seconds from the start of the run; a request is done when
+ * the host sees the event recorded after its call.  Blocks until every
+ * request is done (or timeout_s passes: BK_ERR_SPIN_TIMEOUT).  The workspace
+ * must hold bk_serve_workspace_bytes(requests, mode) and be zeroed once. */
+#define BK_SERVE_SORT 0 /* stable sort_by_key: u32 keys, u32 payload */
+#define BK_SERVE_RBK 1  /* reduce_by_key (equal_to, plus): i32 keys, f32 values */
+#define BK_SERVE_SCAN 2 /* inclusive sum scan: f32, init 0 */
+#define BK_SERVE_PLAIN 0
+#define BK_SERVE_BATCHED 1
+
+typedef struct bk_serve_request {
+  uint32_t kind;       /* BK_SERVE_SORT / _RBK / _SCAN */
+  uint32_t reserved;
+  uint64_t n;          /* elements (> 0) */
+  uint64_t src_offset; /* first element of the input window; a multiple of 4 */
+  double arrival_s;    /* seconds after the start of the run; nondecreasing */
+} bk_serve_request;
+
+typedef struct bk_serve_record {
+  double start_s;  /* issued */
+  double done_s;   /* completion seen by the host */
+  uint64_t out[3]; /* byte offsets in the pool of the request's buffers, in the order above */
+} bk_serve_record;
+
+typedef struct bk_serve_config {
+  const uint32_t *sort_keys; /* sources, source_len elements each */
+  const uint32_t *sort_vals;
+  const int32_t *rbk_keys;
+  const float *rbk_vals;
+  const float *scan_vals;
+  uint64_t source_len;
+  void *pool;                /* device buffer for the requests' buffers (256-byte aligned) */
+  uint64_t pool_bytes;
+  void *ws;                  /* workspace */
+  uint64_t ws_bytes;
+  uint64_t budget_bytes;
+  bk_stream_t stream;
+  int32_t mode;              /* BK_SERVE_PLAIN / BK_SERVE_BATCHED */
+  int32_t max_inflight;      /* batched: batches queued on the stream at once (>= 1) */
+  int32_t keep_buffers;      /* 1: buffers are not reused, so every result stays readable */
+  int32_t reserved;
+  double timeout_s;
+} bk_serve_config;
+
+typedef struct bk_serve_stats {
+  double makespan_s;
+  uint64_t pool_high_water; /* bytes */
+  uint64_t calls;           /* library calls issued */
+  uint64_t batches;         /* of which batched calls */
+} bk_serve_stats;
+
+BK_API uint64_t bk_serve_request_bytes(uint32_t kind, uint64_t n);
+BK_API size_t bk_serve_workspace_bytes(const bk_serve_request *requests, uint32_t count, int mode);
+BK_API int bk_serve_run(const bk_serve_config *cfg, const bk_serve_request *requests, uint32_t count, bk_serve_record *records, bk_serve_stats *stats);
+
+/* The serving loop's pooled allocator on its own (host memory only: it hands
+ * out byte offsets into a buffer of `capacity` bytes).  256-byte granules,
+ * first fit over an address-ordered free list, neighbours coalesced on free.
+ * bk_pool_alloc returns BK_ERR_TOO_LARGE when no free block fits. */
+BK_API void *bk_pool_create(uint64_t capacity);
+BK_API void bk_pool_destroy(void *pool);
+BK_API int bk_pool_alloc(void *pool, uint64_t bytes, uint64_t *offset);
+BK_API int bk_pool_free(void *pool, uint64_t offset);
+BK_API uint64_t bk_pool_in_use(const void *pool);
+BK_API uint64_t bk_pool_high_water(const void *pool);
+BK_API uint32_t bk_pool_free_blocks(const void *pool);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -1,21 +1,25 @@
-"""The serving loop (bulk_b200/serve.py): pooled allocator, request stream,
+"""The serving loop (bk_serve_run in libbulkb200.so, driven by
+bulk_b200/serve.py): pooled allocator, request stream, workspace bound,
 plain vs batched serving, and the alone-vs-in-mix parity of results.
 
-The allocator and the request generator run on CPU tensors; the serving runs
-need a GPU.  Parity: a request's sort result (keys and payload), its
+The allocator (host bookkeeping only), the workspace bound and the request
+generator run without a GPU; the serving runs need one.  Parity: a request's sort result (keys and payload), its
 reduce_by_key keys and count are bit-identical whether it ran alone or inside
 a batch; float sums and scan prefixes agree within the suite's bound
 2*ceil(log2 n)*eps*sum|x| (twice, since both sides carry that error).
 """
 from __future__ import annotations
 
+import ctypes
 import math
 
 import numpy as np
 import pytest
 import torch
 
-from bulk_b200 import serve
+import bulk_b200
+from bulk_b200 import _lib, serve
+from bulk_b200.batch import batch_workspace_bytes
 
 
 def test_pool_first_fit_coalesces_and_tracks_use():
@@ -39,7 +43,7 @@ def test_pool_first_fit_coalesces_and_tracks_use():
             live[off] = n
     for off in list(live):
         pool.free(off)
-    assert pool.in_use == 0 and pool._free == [(0, pool.capacity)]
+    assert pool.in_use == 0 and pool.free_blocks() == 1
     assert pool.high_water > 0
 
 
@@ -50,6 +54,44 @@ def test_pool_refuses_when_full_and_views_alias_the_buffer():
     v = pool.view(a, 10, torch.int32)
     v[:] = 7
     assert pool.buf[a:a + 40].view(torch.int32).tolist() == [7] * 10
+
+
+def test_pool_rejects_unknown_offsets_and_frees_coalesce_both_ways():
+    pool = serve.DevicePool(1 << 16, device="cpu")
+    a, b, c = pool.alloc(1000), pool.alloc(1000), pool.alloc(1000)
+    assert (a, b, c) == (0, 1024, 2048)
+    with pytest.raises(bulk_b200.BulkError):
+        pool.free(12345)
+    pool.free(a)
+    pool.free(c)  # c merges with the tail
+    assert pool.free_blocks() == 2
+    pool.free(b)  # b merges with both neighbours
+    assert pool.free_blocks() == 1 and pool.in_use == 0 and pool.high_water == 3072
+
+
+def _req_array(reqs):
+    arr = (serve._Request * len(reqs))()
+    for i, (k, n) in enumerate(reqs):
+        arr[i].kind, arr[i].n = k, n
+    return arr
+
+
+def test_workspace_bound_covers_every_call():
+    """Plain: the largest single-call workspace.  Batched: at least every
+    kind's largest batch of BK_BATCH_MAX requests, and never less than plain
+    needs for a one-request batch."""
+    ws = bulk_b200.workspace_bytes
+    rng = np.random.default_rng(3)
+    reqs = [(int(k), int(n)) for k, n in zip(rng.integers(0, 3, 700), rng.integers(1, 1 << 22, 700))]
+    arr = _req_array(reqs)
+    plain = _lib.lib.bk_serve_workspace_bytes(ctypes.cast(arr, ctypes.c_void_p), len(reqs), 0)
+    singles = {0: ("sort_by_key", "u32", "u32"), 1: ("reduce_by_key", "i32", "f32"), 2: ("inclusive_scan", "f32", None)}
+    assert plain == max(ws(*singles[k], n) for k, n in reqs)
+    batched = _lib.lib.bk_serve_workspace_bytes(ctypes.cast(arr, ctypes.c_void_p), len(reqs), 1)
+    for kind in range(3):
+        top = sorted((n for k, n in reqs if k == kind), reverse=True)[:256]
+        assert batched >= batch_workspace_bytes(*singles[kind], top)
+    assert batched >= plain
 
 
 def test_request_stream_follows_the_config():
@@ -99,7 +141,11 @@ def test_serving_results_match_each_request_alone(cuda, mode):
     reqs = serve.make_requests(120, math.inf, seed=77, lo=1 << 10, hi=1 << 18)
     stats = server.run(reqs, mode)
     assert stats["requests"] == 120 and stats["req_per_s"] > 0
-    assert pool.in_use == 0 and server.admitted_bytes == 0
+    assert all(0 <= r.arrival <= r.start <= r.done for r in reqs)
+    if mode == "plain":
+        assert stats["calls"] == 120 and stats["batches"] == 0
+    else:
+        assert 3 <= stats["batches"] < 120  # all 120 arrive at once: few batches
     torch.cuda.synchronize()
     for r in reqs:
         got = server.results[r.rid]
@@ -128,4 +174,17 @@ def test_admission_respects_the_budget(cuda):
     reqs = serve.make_requests(60, math.inf, seed=5, lo=1 << 12, hi=1 << 18)
     stats = server.run(reqs, "batched")
     assert stats["requests"] == 60
-    assert pool.high_water <= budget + 60 * 3 * 256  # granule rounding
+    assert 0 < stats["pool_high_water_bytes"] <= budget + 60 * 3 * 256  # granule rounding
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["plain", "batched"])
+def test_a_request_larger_than_the_budget_runs_alone(cuda, mode):
+    src = serve.Sources(1 << 18)
+    pool = serve.DevicePool(1 << 26)
+    server = serve.Server(src, pool, budget_bytes=1 << 20)
+    reqs = serve.make_requests(30, math.inf, seed=9, lo=1 << 16, hi=1 << 18)  # 0.5-2 MB each
+    stats = server.run(reqs, mode)
+    assert stats["requests"] == 30 and all(r.done >= r.start >= 0 for r in reqs)
+    big = max(r.nbytes() for r in reqs)
+    assert big > 1 << 20 and stats["pool_high_water_bytes"] <= (1 << 20) + big
