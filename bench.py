@@ -17,8 +17,8 @@ ops    = per-op GB/s: the headline's six calls, and the other benchmark
          2^26 u32/u64 keys with u32 payload, reduce_by_key 2^27 i32 keys with
          geometric / Zipf runs and f32 / f64 values), timed after the headline.
 
-serving = plain vs batched serving of a mixed request stream (bulk_b200/serve.py:
-         40% sort_by_key u32/u32, 30% reduce_by_key i32/f32, 30% scan f32;
+serving = plain vs batched serving of a mixed request stream (the native loop
+         bk_serve_run, driven by bulk_b200/serve.py: 40% sort_by_key u32/u32, 30% reduce_by_key i32/f32, 30% scan f32;
          sizes log-uniform in [2^10, 2^24], and a small-request variant in
          [2^10, 2^16]): saturation req/s and, at 2000 req/s Poisson arrivals,
          p50/p99 latency, for one call per request ("plain") and continuous
@@ -414,17 +414,20 @@ def other_ops(device, peak, quick=False, shift=0):
             k.copy_(k0)
             v.copy_(v0)
         ms = _time_op(lambda: bulk_b200.stable_sort_by_key(k, v), prep=prep, reps=reps)
-        byts = 2 * n * (k0.element_size() + 4)
-        passes = 0
-        w = 8192 if tag == "u32" else 4096
-        while w < n:
-            w *= 2
-            passes += 1
+        ksz = k0.element_size()
+        byts = 2 * n * (ksz + 4)
+        # LSD radix: one pass per key byte; a pass reads the keys (digit
+        # counts), then reads and writes keys and payloads (scatter), plus the
+        # digit counts (n / 4096 tiles x 256 u32) written, scanned and read
+        passes = ksz
+        counts = (n + 4095) // 4096 * 256 * 4
+        moved = passes * (n * ksz + 2 * n * (ksz + 4) + 4 * counts)
         res[f"sort_by_key_{tag}_u32_2^{26 - shift}"] = {
             "ms": ms, "GBps": byts / ms / 1e6, "frac_of_hbm": byts / ms / 1e6 / peak, "algorithmic_bytes": byts,
-            "merge_passes": passes,
-            "bytes_moved_by_design": (passes + 1) * byts,
-            "GBps_of_bytes_moved": (passes + 1) * byts / ms / 1e6}
+            "radix_passes": passes,
+            "bytes_moved_by_design": moved,
+            "GBps_of_bytes_moved": moved / ms / 1e6,
+            "frac_of_hbm_by_design": moved / ms / 1e6 / peak}
         del k0, v0, k, v
 
     # reduce_by_key: 2^27 pairs, i32 keys in runs (geometric mean 16 / Zipf 1.2 cap 2^20), f32/f64 U[0,1)
