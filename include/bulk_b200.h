@@ -169,13 +169,17 @@ BK_API int bk_merge_by_key_f32_u64(const float *a_keys, const uint64_t *a_vals, 
 BK_API int bk_merge_by_key_f64_u32(const double *a_keys, const uint32_t *a_vals, uint64_t na, const double *b_keys, const uint32_t *b_vals, uint64_t nb, double *out_keys, uint32_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_merge_by_key_f64_u64(const double *a_keys, const uint64_t *a_vals, uint64_t na, const double *b_keys, const uint64_t *b_vals, uint64_t nb, double *out_keys, uint64_t *out_vals, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
-/* ---- stable sort by key (merge sort) --------------------------------------
+/* ---- stable sort by key -----------------------------------------------------
  * In-place stable sort of keys[0..n) under operator<, moving vals with their
- * keys; equal keys keep their input order.  Replaces
- * stable_merge_sort_by_key(keys_first, keys_last, values_first, comp),
- * merge_sort_by_key.cu:150-209 (block sort bulk/algorithm/sort.hpp:152-166,
- * stable_merge_sort.hpp:125-206, then merge-path passes).  Keys must not be
- * NaN.  bk_sort_keys_* sorts keys alone. */
+ * keys; equal keys keep their input order (-0.0 and +0.0 are equal).
+ * Replaces stable_merge_sort_by_key(keys_first, keys_last, values_first,
+ * comp), merge_sort_by_key.cu:150-209 (block sort bulk/algorithm/sort.hpp:
+ * 152-166, stable_merge_sort.hpp:125-206, then merge-path passes).  The
+ * stable order is unique, so the result is the reference's whichever way it
+ * is computed: one block sort for an array of one tile (8192 4-byte / 4096
+ * 8-byte keys), a stable LSD radix sort below 2^30 elements, block sort and
+ * merge-path passes from 2^30 on.  Keys must not be NaN.  bk_sort_keys_*
+ * sorts keys alone. */
 BK_API int bk_sort_keys_i32(int32_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_sort_keys_u32(uint32_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_sort_keys_i64(int64_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
