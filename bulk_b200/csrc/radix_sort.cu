@@ -27,6 +27,8 @@
 // A batch lays its arrays' count regions one after another, so the one scan
 // serves all of them: an array's positions are the scanned values minus the
 // number of elements of the arrays before it.
+#include <type_traits>
+
 #include "bk_common.cuh"
 #include "bk_merge.cuh"  // NoPayload, has_payload, payload_bytes
 #include "bulk_b200.h"
@@ -238,89 +240,105 @@ __global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downswe
   for (int i = tid; i < WARPS * kRsBins; i += TH) (&s_whist[0][0])[i] = 0u;
   __syncthreads();
 
-  K k[ITEMS];
-  P v[ITEMS];
-  auto elem = [&](int j) { return warp * 32 * ITEMS + j * 32 + lane; };
-  // digit of item j, recomputed where needed.  Past the tile's end it is
-  // 255: those items come after every real one in (warp, item, lane) order,
-  // so they rank last in the tile and are never written out.
-  auto digit_of = [&](int j) { return elem(j) < count ? rs_digit(k[j], shift) : kRsBins - 1; };
+  // The tile body, compiled twice: for full tiles (no bounds checks) and for
+  // an array's last, partial tile.
+  auto body = [&](auto full_tag) {
+    constexpr bool FULL = decltype(full_tag)::value;
+    K k[ITEMS];
+    P v[ITEMS];
+    auto elem = [&](int j) { return warp * 32 * ITEMS + j * 32 + lane; };
 #pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    const bool ok = elem(j) < count;
-    k[j] = ok ? in_k[tbase + elem(j)] : K();
-    if constexpr (has_payload<P>()) v[j] = ok ? in_v[tbase + elem(j)] : P();
-  }
-  // rank within the warp: keys of one digit in input order (a rank is below
-  // 512, so two share a register).  The lowest lane of each digit reserves
-  // the digit's keys in the warp's counter; the shuffle that hands the old
-  // count to the other lanes also orders item j's atomic before item j+1's.
-  unsigned int rank2[ITEMS / 2];
-  const unsigned int lt = (1u << lane) - 1u;
-  unsigned int pm[V == 1 ? ITEMS : 1];
-  if constexpr (V == 1) {
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) pm[j] = rs_peers((unsigned int)digit_of(j));
-  }
-#pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    const int dj = digit_of(j);
-    unsigned int peers;
-    if constexpr (V == 1) peers = pm[j];
-    else peers = rs_peers((unsigned int)dj);
-    const int leader = __ffs(peers) - 1;
-    unsigned int before = 0;
-    if (lane == leader) before = atomicAdd(&s_whist[warp][dj], (unsigned int)__popc(peers));
-    before = __shfl_sync(0xffffffffu, before, leader);
-    const unsigned int r = before + __popc(peers & lt);
-    if (j & 1) rank2[j >> 1] |= r << 16;
-    else rank2[j >> 1] = r;
-  }
-  __syncthreads();
-
-  // thread d < 256: the digit's tile count, then its start in the staged
-  // tile for each warp (the tile's exclusive count plus the warps before)
-  const int d = tid;
-  unsigned int cnt = 0;
-  if (d < kRsBins) {
-#pragma unroll
-    for (int w = 0; w < WARPS; ++w) cnt += s_whist[w][d];
-  }
-  unsigned int tile_total;
-  const unsigned int tile_excl = block_exclusive_scan<TH>(cnt, OpSum<unsigned int>(), s_scan, tile_total);
-  if (d < kRsBins) {
-    unsigned int run = tile_excl;
-#pragma unroll
-    for (int w = 0; w < WARPS; ++w) {
-      const unsigned int c = s_whist[w][d];
-      s_whist[w][d] = run;
-      run += c;
+    for (int j = 0; j < ITEMS; ++j) {
+      const bool ok = FULL || elem(j) < count;
+      k[j] = ok ? in_k[tbase + elem(j)] : K();
+      if constexpr (has_payload<P>()) v[j] = ok ? in_v[tbase + elem(j)] : P();
     }
-    if (d == kRsBins - 1) cnt -= (unsigned int)(kRsTile - count);  // real keys of digit 255
-    const unsigned int incl = scanned[tl.count_base + (uint64_t)d * tl.tiles + tl.local];
-    s_dst[d] = incl - cnt - tl.elem_base - tile_excl;
-  }
-  __syncthreads();
-
-  // stage in digit order
+    // the items' digits, four to a register.  Past the tile's end the digit
+    // is 255: those items come after every real one in (warp, item, lane)
+    // order, so they rank last in the tile and are never written out.
+    uint32_t dig4[ITEMS / 4];
 #pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    const int dj = digit_of(j);
-    const unsigned int rank = (rank2[j >> 1] >> (16 * (j & 1))) & 0xffffu;
-    const unsigned int pos = s_whist[warp][dj] + rank;
-    sk[pos] = k[j];
-    if constexpr (has_payload<P>()) sv[pos] = v[j];
-  }
-  __syncthreads();
-  // write out: position p of the staged tile goes to s_dst[digit] + p
-  for (int p = tid; p < count; p += TH) {
-    const K key = sk[p];
-    const uint64_t g = (uint64_t)(s_dst[rs_digit(key, shift)] + (unsigned int)p);
-    if (g < tl.n) {  // always true when the counts are consistent
-      out_k[g] = key;
-      if constexpr (has_payload<P>()) out_v[g] = sv[p];
+    for (int j = 0; j < ITEMS; ++j) {
+      const uint32_t dj = (FULL || elem(j) < count) ? (uint32_t)rs_digit(k[j], shift) : kRsBins - 1u;
+      if (j & 3) dig4[j >> 2] |= dj << (8 * (j & 3));
+      else dig4[j >> 2] = dj;
     }
-  }
+    auto digit_of = [&](int j) { return (int)((dig4[j >> 2] >> (8 * (j & 3))) & 0xffu); };
+    // rank within the warp: keys of one digit in input order (a rank is
+    // below 512, so two share a register).  The lowest lane of each digit
+    // reserves the digit's keys in the warp's counter; the shuffle that hands
+    // the old count to the other lanes also orders item j's atomic before
+    // item j+1's.
+    unsigned int rank2[ITEMS / 2];
+    const unsigned int lt = (1u << lane) - 1u;
+    unsigned int pm[V == 1 ? ITEMS : 1];
+    if constexpr (V == 1) {
+#pragma unroll
+      for (int j = 0; j < ITEMS; ++j) pm[j] = rs_peers((unsigned int)digit_of(j));
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const int dj = digit_of(j);
+      unsigned int peers;
+      if constexpr (V == 1) peers = pm[j];
+      else peers = rs_peers((unsigned int)dj);
+      const int leader = __ffs(peers) - 1;
+      unsigned int before = 0;
+      if (lane == leader) before = atomicAdd(&s_whist[warp][dj], (unsigned int)__popc(peers));
+      before = __shfl_sync(0xffffffffu, before, leader);
+      const unsigned int r = before + __popc(peers & lt);
+      if (j & 1) rank2[j >> 1] |= r << 16;
+      else rank2[j >> 1] = r;
+    }
+    __syncthreads();
+
+    // thread d < 256: the digit's tile count, then its start in the staged
+    // tile for each warp (the tile's exclusive count plus the warps before)
+    const int d = tid;
+    unsigned int cnt = 0;
+    if (d < kRsBins) {
+#pragma unroll
+      for (int w = 0; w < WARPS; ++w) cnt += s_whist[w][d];
+    }
+    unsigned int tile_total;
+    const unsigned int tile_excl = block_exclusive_scan<TH>(cnt, OpSum<unsigned int>(), s_scan, tile_total);
+    if (d < kRsBins) {
+      unsigned int run = tile_excl;
+#pragma unroll
+      for (int w = 0; w < WARPS; ++w) {
+        const unsigned int c = s_whist[w][d];
+        s_whist[w][d] = run;
+        run += c;
+      }
+      if (!FULL && d == kRsBins - 1) cnt -= (unsigned int)(kRsTile - count);  // real keys of digit 255
+      const unsigned int incl = scanned[tl.count_base + (uint64_t)d * tl.tiles + tl.local];
+      s_dst[d] = incl - cnt - tl.elem_base - tile_excl;
+    }
+    __syncthreads();
+
+    // stage in digit order
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const int dj = digit_of(j);
+      const unsigned int rank = (rank2[j >> 1] >> (16 * (j & 1))) & 0xffffu;
+      const unsigned int pos = s_whist[warp][dj] + rank;
+      sk[pos] = k[j];
+      if constexpr (has_payload<P>()) sv[pos] = v[j];
+    }
+    __syncthreads();
+    // write out: position p of the staged tile goes to s_dst[digit] + p
+#pragma unroll 4
+    for (int p = tid; p < (FULL ? kRsTile : count); p += TH) {
+      const K key = sk[p];
+      const uint64_t g = (uint64_t)(s_dst[rs_digit(key, shift)] + (unsigned int)p);
+      if (g < tl.n) {  // always true when the counts are consistent
+        out_k[g] = key;
+        if constexpr (has_payload<P>()) out_v[g] = sv[p];
+      }
+    }
+  };
+  if (count == kRsTile) body(std::true_type{});
+  else body(std::false_type{});
 }
 
 template <typename K, typename P>
