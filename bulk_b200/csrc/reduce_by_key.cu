@@ -64,9 +64,22 @@ template <typename K, typename V>
 size_t rbk_num_tiles(uint64_t n) {
   return (size_t)((n + RbkCfg<K, V>::TILE - 1) / RbkCfg<K, V>::TILE);
 }
+// Workspace: the header, one look-back status per tile, then the tail-mark
+// ring: three tile-sized value slots per persistent CTA (phase 1 of a tile
+// writes its tails' values there; the re-read for phase 2 brings them back).
+constexpr size_t kRbkMaxGrid = 320;  // persistent CTAs at most (2 per SM)
+template <typename K, typename V>
+size_t rbk_ring_offset(size_t tiles) {
+  return align_up(kHeaderBytes + RbkCfg<K, V>::Status::bytes(tiles), 256);
+}
+template <typename K, typename V>
+size_t rbk_ws_for_tiles(size_t tiles) {
+  const size_t slots = 3 * (tiles < kRbkMaxGrid ? tiles : kRbkMaxGrid);
+  return rbk_ring_offset<K, V>(tiles) + slots * RbkCfg<K, V>::TILE * sizeof(V);
+}
 template <typename K, typename V>
 size_t rbk_ws_bytes(uint64_t n) {
-  return kHeaderBytes + RbkCfg<K, V>::Status::bytes(rbk_num_tiles<K, V>(n));
+  return rbk_ws_for_tiles<K, V>(rbk_num_tiles<K, V>(n));
 }
 
 template <typename Status>
@@ -198,6 +211,44 @@ __device__ __forceinline__ void rbk_sync_load(const K *keys, const V *vals, uint
   }
 }
 
+// Leader: re-read tile `tile` for phase 2 into buffer `buf`: its keys from
+// the input (L2) and its tails' values from the mark slot `marks` (TILE
+// values, 16-byte aligned).  Returns whether a TMA copy was issued on `bar`;
+// without TMA (keys not 16-byte aligned) the compute warps copy both.
+template <typename K, typename V>
+__device__ __forceinline__ bool rbk_issue_reload(const K *keys, const V *marks, uint64_t n, unsigned int tile,
+                                                 unsigned char *buf, uint64_t *bar, uint64_t policy, bool tma_ok) {
+  using C = RbkCfg<K, V>;
+  constexpr uint32_t KC = 16 / sizeof(K);
+  if (!tma_ok) return false;
+  const uint64_t base = (uint64_t)tile * C::TILE;
+  const uint32_t count = (uint32_t)((n - base) < (uint64_t)C::TILE ? (n - base) : (uint64_t)C::TILE);
+  K *sk = reinterpret_cast<K *>(buf);
+  V *sv = reinterpret_cast<V *>(buf + C::KEY_BYTES);
+  const uint32_t bk = count & ~(KC - 1);
+  for (uint32_t i = bk; i < count; ++i) sk[i] = keys[base + i];
+  const uint32_t vbytes = (uint32_t)align_up(count * sizeof(V), 16);  // within the slot
+  mbar_arrive_expect_tx(bar, bk * (uint32_t)sizeof(K) + vbytes);
+  if (bk) tma_load_1d_hint(sk, keys + base, bk * (uint32_t)sizeof(K), bar, policy);
+  tma_load_1d_hint(sv, marks, vbytes, bar, policy);
+  return true;
+}
+
+// Compute threads: plain copy of a tile's keys and tail marks for phase 2.
+template <typename K, typename V>
+__device__ __forceinline__ void rbk_sync_reload(const K *keys, const V *marks, uint64_t n, unsigned int tile,
+                                                unsigned char *buf) {
+  using C = RbkCfg<K, V>;
+  const uint64_t base = (uint64_t)tile * C::TILE;
+  const uint32_t count = (uint32_t)((n - base) < (uint64_t)C::TILE ? (n - base) : (uint64_t)C::TILE);
+  K *sk = reinterpret_cast<K *>(buf);
+  V *sv = reinterpret_cast<V *>(buf + C::KEY_BYTES);
+  for (uint32_t i = threadIdx.x; i < count; i += kRbkWarps * 32) {
+    sk[i] = keys[base + i];
+    sv[i] = marks[i];
+  }
+}
+
 // Loads a lane's B bytes (B = 32 or 64: C = B/16 chunks of 16 bytes) starting
 // at byte offset lane_off of `base` into dst, conflict-free: eight lanes share
 // one 128-byte bank period, so lane l fetches its chunks starting at chunk
@@ -308,34 +359,43 @@ __device__ __forceinline__ void rbk_flags(const unsigned char *buf, const K (*hb
   lr.tail = tail;
 }
 
-// (c, v) of a lane's elements folded in order.
+// (c, v) of a lane's elements folded in order.  At every tail the run's value
+// so far -- from the run's head, or from the lane's first element when the
+// run began before the lane -- goes to the lane's tail-mark slot (marks[j]
+// for element j), where the re-read for phase 2 picks it up.
 template <typename K, typename V, int M>
-__device__ __forceinline__ Seg<V> lane_fold(const LaneRun<K, V, M> &lr) {
+__device__ __forceinline__ Seg<V> lane_fold_mark(const LaneRun<K, V, M> &lr, V *marks) {
   uint32_t c = __popc(lr.head);
   V v = V(0);
 #pragma unroll
   for (int j = 0; j < M; ++j) {
     if (lr.head & (1u << j)) v = lr.val[j];
     else v = (V)(v + lr.val[j]);
+    if (lr.tail & (1u << j)) marks[j] = v;
   }
   return Seg<V>{c, v};
 }
 
 // Persistent two-phase reduce_by_key; the roles, buffer rotation and
 // hand-over protocol are scan_kernel's (scan.cu), with these differences: a
-// buffer holds a tile's keys, values and halo keys; phase 2 only reads its
-// buffer (the runs go straight to out_keys / out_vals), so the loader reuses
-// a buffer once the compute warps are done reading it, with no store to
-// drain; and without TMA (pointers not 16-byte aligned) the compute warps
-// stage both tiles themselves between two compute-only barriers.
+// buffer holds a tile's keys, values and halo keys; phase 1 also writes each
+// tail's value so far to the CTA's tail-mark slot for the tile (ring slot
+// blockIdx.x * 3 + iteration mod 3), and the re-read for phase 2 brings back
+// the tile's keys with those marks in place of its values, so phase 2 costs
+// one step per run, not per element; phase 2 only reads its buffer (the runs
+// go straight to out_keys / out_vals), so the loader reuses a buffer once the
+// compute warps are done reading it, with no store to drain; and without TMA
+// (pointers not 16-byte aligned) the compute warps stage both tiles
+// themselves between two compute-only barriers.
 template <typename K, typename V, typename Src>
 __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_constant__ Src src,
                                                              typename RbkCfg<K, V>::Status st, WsHeader *hdr,
-                                                             unsigned long long spin_limit_ns,
+                                                             V *ring, unsigned long long spin_limit_ns,
                                                              long long skip_publish_tile, unsigned int num_tiles) {
   using C = RbkCfg<K, V>;
   using P = typename C::P;
   constexpr int M = C::M, TILE = C::TILE, NB = kRbkBufs, Q = kRbkQueue;
+  V *const cta_ring = ring + (size_t)blockIdx.x * 3 * TILE;  // this CTA's three tail-mark slots
   constexpr unsigned int NONE = 0xffffffffu;
   OpSeg<V> op;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -346,6 +406,7 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
   __shared__ __align__(8) uint64_t s_qbar[Q];
   __shared__ unsigned int s_ticket[NB];
   __shared__ P s_wagg[4][kRbkWarps];  // per-warp (c, v) of t_i, by iteration mod 4
+  __shared__ P s_wexcl[4][kRbkWarps];  // the warps before each warp, folded (thread 0)
   // phase 1's per-lane results, kept for phase 2 (each warp reads back only
   // its own lanes, so program order protects them; by iteration mod 3):
   // head flags | tail flags << 16, and the lane's exclusive (c, v) in its warp
@@ -424,9 +485,10 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
       }
       p1par[bt] ^= 1u;
       tx = false;
-      if (q_tile != NONE) {
+      if (q_tile != NONE) {  // t_{it-1}: its phase 1 ran in iteration it-1
         const RbkTile<K, V> tl = src.tile(q_tile);
-        tx = rbk_issue_load<K, V>(tl.keys, tl.vals, tl.n, tl.local, buf(bt), s_halo[bt], &s_full[bt], stream, tl.tma);
+        tx = rbk_issue_reload<K, V>(tl.keys, cta_ring + (size_t)((it + 2) % 3) * TILE, tl.n, tl.local, buf(bt),
+                                    &s_full[bt], stream, tl.tma);
       }
       if (!tx) mbar_arrive(&s_full[bt]);
       ++armed[bt];
@@ -523,9 +585,9 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
         const RbkTile<K, V> tl = src.tile(t);
         if (!tl.tma) rbk_sync_load<K, V>(tl.keys, tl.vals, tl.n, tl.local, buf(bt));
       }
-      if (p != NONE) {
+      if (p != NONE) {  // t_{it-2}: its phase 1 ran in iteration it-2
         const RbkTile<K, V> tl = src.tile(p);
-        if (!tl.tma) rbk_sync_load<K, V>(tl.keys, tl.vals, tl.n, tl.local, buf(bp));
+        if (!tl.tma) rbk_sync_reload<K, V>(tl.keys, cta_ring + (size_t)((it + 1) % 3) * TILE, tl.n, tl.local, buf(bp));
       }
       named_barrier_sync(2, 32 * kRbkWarps);
     }
@@ -535,7 +597,9 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
       LaneRun<K, V, M> lr;
       rbk_load_lane<K, V>(buf(bt), count, warp, lane, lr);
       rbk_flags<K, V>(buf(bt), s_halo[bt], count, tl.first(), tl.last(), warp, lane, lr);
-      const P incl = warp_inclusive_scan(lane_fold(lr), op, lane);
+      V *marks = cta_ring + (size_t)(it % 3) * TILE + (warp * 32 + lane) * M;
+      const P incl = warp_inclusive_scan(lane_fold_mark(lr, marks), op, lane);
+      fence_proxy_async_global();  // the marks are read back by a TMA copy
       if (lane == 31) s_wagg[it & 3][warp] = incl;
       P lex = shfl_up(incl, 1);
       if (lane == 0) lex = OpSeg<V>::identity();
@@ -553,7 +617,10 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
       P agg = OpSeg<V>::identity();
       if (t != NONE) {
 #pragma unroll
-        for (int i = 0; i < kRbkWarps; ++i) agg = op(agg, s_wagg[it & 3][i]);
+        for (int i = 0; i < kRbkWarps; ++i) {
+          s_wexcl[it & 3][i] = agg;
+          agg = op(agg, s_wagg[it & 3][i]);
+        }
         if ((long long)t != skip_publish_tile) st.publish(t, src.tile(t).first() ? kStPrefix : kStAggregate, agg);
       }
       s_q_tile[it % Q] = t;
@@ -573,31 +640,29 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
       const unsigned int e = (unsigned int)it - 2u;
       const RbkTile<K, V> tl = src.tile(p);
       const uint32_t count = tl.count();
-      const bool last_tile = tl.last();
-      LaneRun<K, V, M> lr;
-      rbk_load_lane<K, V>(buf(bp), count, warp, lane, lr);
       const int sl = (it + 1) % 3, li = warp * 32 + lane;  // phase 1 of p ran at it - 2
       const uint32_t fl = s_lflags[sl][li];
       const uint32_t head = fl & 0xffffu, tail = fl >> 16;
-      P carry = s_q_prefix[e % Q];
-      for (int i = 0; i < warp; ++i) carry = op(carry, s_wagg[(it + 2) & 3][i]);
-      carry = op(carry, P{s_lc[sl][li], s_lv[sl][li]});
-      // walk the lane's elements with the running (c, v); each tail emits its
-      // run (elements past the tile's end have no flags and value 0)
-      uint32_t c = carry.c;
-      V v = carry.v;
-#pragma unroll
-      for (int j = 0; j < M; ++j) {
-        const bool h = (head >> j) & 1u;
-        c += h ? 1u : 0u;
-        v = h ? lr.val[j] : (V)(v + lr.val[j]);
-        if ((tail >> j) & 1u) {
-          tl.out_keys[c - 1] = lr.key[j];
+      const uint32_t e0 = (uint32_t)li * M;
+      const bool holds_last = tl.last() && e0 < count && count <= e0 + M;  // the input's last element
+      if (tail != 0u || holds_last) {
+        P carry = op(s_q_prefix[e % Q], s_wexcl[(it + 2) & 3][warp]);
+        carry = op(carry, P{s_lc[sl][li], s_lv[sl][li]});
+        // each tail: its key, and its mark (the run's value from its head, or
+        // from the lane's first element when the run began before the lane)
+        const K *sk = reinterpret_cast<const K *>(buf(bp)) + e0;
+        const V *sv = reinterpret_cast<const V *>(buf(bp) + C::KEY_BYTES) + e0;
+        for (uint32_t tb = tail; tb != 0u; tb &= tb - 1u) {
+          const int j = __ffs(tb) - 1;
+          const uint32_t upto = head & ((2u << j) - 1u);  // heads at or before j
+          const uint32_t c = carry.c + (uint32_t)__popc(upto);
+          V v = sv[j];
+          if (upto == 0u) v = (V)(carry.v + v);
+          tl.out_keys[c - 1] = sk[j];
           tl.out_vals[c - 1] = v;
         }
+        if (holds_last) *tl.num_out = carry.c + (uint32_t)__popc(head);
       }
-      const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
-      if (last_tile && e0 < count && count <= e0 + M) *tl.num_out = c;  // this lane holds the input's last element
     }
     __syncwarp();
     if (!bad && lane == 0) mbar_arrive(&s_p2[bp]);
@@ -617,7 +682,7 @@ int rbk_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStrea
   int st = host::device_info(&di);
   if (st != BK_OK) return st;
   if (tiles >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
-  st = host::check_ws(d_ws, ws_bytes, kHeaderBytes + C::Status::bytes(tiles));
+  st = host::check_ws(d_ws, ws_bytes, rbk_ws_for_tiles<K, V>(tiles));
   if (st != BK_OK) return st;
   WsHeader *hdr = reinterpret_cast<WsHeader *>(d_ws);
   auto status = C::Status::at(reinterpret_cast<char *>(d_ws) + kHeaderBytes, tiles);
@@ -632,8 +697,9 @@ int rbk_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStrea
     if ((st = host::set_smem_attrs(rbk_kernel<K, V, Src>, smem)) != BK_OK) return st;
     attr_set = true;
   }
-  const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * 2);
-  rbk_kernel<K, V, Src><<<grid, kRbkThreads, smem, stream>>>(src, status, hdr, limit, dbg.skip_publish_tile,
+  const unsigned grid = (unsigned)std::min<size_t>(tiles, std::min<size_t>((size_t)di.sm_count * 2, kRbkMaxGrid));
+  V *ring = reinterpret_cast<V *>(reinterpret_cast<char *>(d_ws) + rbk_ring_offset<K, V>(tiles));
+  rbk_kernel<K, V, Src><<<grid, kRbkThreads, smem, stream>>>(src, status, hdr, ring, limit, dbg.skip_publish_tile,
                                                             (unsigned)tiles);
   return host::launch_status();
 }
@@ -717,7 +783,7 @@ template <typename K, typename V>
 size_t rbk_batch_ws(const uint64_t *sizes, uint32_t count) {
   size_t tiles = 0;
   for (uint32_t i = 0; i < count; ++i) tiles += rbk_num_tiles<K, V>(sizes[i]);
-  return kHeaderBytes + RbkCfg<K, V>::Status::bytes(tiles);
+  return rbk_ws_for_tiles<K, V>(tiles);
 }
 
 size_t rbk_batch_workspace_bytes(int key_dtype, int value_dtype, const uint64_t *sizes, uint32_t count) {
