@@ -72,6 +72,19 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def whole_job(ms_step, bytes_step, world, device=None):
+    """(ms per step, whole-job GB/s): the step time is the slowest rank's (a
+    MAX all-reduce when world > 1, so every rank must call it), and every rank
+    processed bytes_step per step."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([ms_step], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    return ms_step, bytes_step * world / (ms_step * 1e-3) / 1e9
+
+
 def _env_rank():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
             int(os.environ.get("LOCAL_RANK", 0)))
@@ -493,14 +506,9 @@ def main(argv=None):
     import bulk_b200  # noqa: F401  (fails loudly without the CUDA library)
 
     ms, per, clocks, xs = headline(args, device, rank, world)
-    ms_step = ms / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
     n = args.n
     bytes_step = sum(3 * n * s for _, s in DTYPES)
-    value = bytes_step * world / (ms_step * 1e-3) / 1e9
+    ms_step, value = whole_job(ms / args.steps, bytes_step, world, device)
     peak, peak_kind = _peaks()
 
     # dominant kernel: the call with the largest mean time
