@@ -162,6 +162,20 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 }
 
 // Record the first device-side error in the workspace header.
+// Asks L2 to fetch [p, p + bytes) from memory ahead of its use (nothing
+// reaches the SM).  The range is trimmed inward to 16-byte boundaries, so the
+// prefetch never leaves the caller's array.
+__device__ __forceinline__ void prefetch_l2_range(const void *p, uint64_t bytes) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  uintptr_t lo = (a + 15) & ~(uintptr_t)15;
+  const uintptr_t hi = (a + bytes) & ~(uintptr_t)15;
+  while (lo < hi) {
+    const uint32_t s = (hi - lo) > (1u << 30) ? (1u << 30) : (uint32_t)(hi - lo);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(s) : "memory");
+    lo += s;
+  }
+}
+
 __device__ __forceinline__ void record_error(WsHeader *h, int code, unsigned int tile) {
   if (atomicCAS(&h->status, 0, code) == 0) atomicExch(&h->err_tile, tile);
 }
@@ -297,6 +311,16 @@ struct DeviceInfo {
 
 // Cached per device; thread-safe (call_once per slot).
 int device_info(DeviceInfo *out);
+
+// CTAs of `kern` (threads, dynamic shared memory) resident on the whole GPU
+// at once: how far ahead of itself a CTA can usefully prefetch.
+template <typename Kern>
+inline uint64_t resident_ctas(Kern kern, int threads, size_t smem, int sm_count) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return (uint64_t)per_sm * (uint64_t)sm_count;
+}
 
 // Debug settings (process-wide, test-only).
 struct DebugFault {

@@ -38,14 +38,28 @@ __global__ void merge_partition_kernel(const K *a, uint64_t na, const K *b, uint
   parts[k] = merge_path<K, uint64_t>(a, na, b, nb, diag);
 }
 
+// One CTA per output tile.  Thread 0 first asks L2 for the inputs of tile
+// k + ahead (the CTA that will start about when every CTA now resident has
+// finished), so that CTA's loads hit L2 instead of waiting on memory.
 template <typename K, typename P>
 __global__ void __launch_bounds__(kMergeThreads, 4) merge_kernel(const K *a, const P *av, uint64_t na, const K *b,
                                                               const P *bv, uint64_t nb, K *out, P *outv,
-                                                              const uint64_t *parts) {
+                                                              const uint64_t *parts, uint64_t ahead) {
   constexpr int TILE = MergeCfg<K>::TILE;
   extern __shared__ __align__(16) unsigned char smem[];
   const uint64_t k = blockIdx.x;
   const uint64_t total = na + nb;
+  if (threadIdx.x == 0 && k + ahead < gridDim.x) {
+    const uint64_t f = k + ahead;
+    const uint64_t e0 = f * TILE, e1 = e0 + TILE < total ? e0 + TILE : total;
+    const uint64_t fa0 = parts[f], fa1 = parts[f + 1], fb0 = e0 - fa0, fb1 = e1 - fa1;
+    prefetch_l2_range(a + fa0, (fa1 - fa0) * sizeof(K));
+    prefetch_l2_range(b + fb0, (fb1 - fb0) * sizeof(K));
+    if constexpr (has_payload<P>()) {
+      prefetch_l2_range(av + fa0, (fa1 - fa0) * sizeof(P));
+      prefetch_l2_range(bv + fb0, (fb1 - fb0) * sizeof(P));
+    }
+  }
   const uint64_t d0 = k * TILE;
   const uint64_t d1 = d0 + TILE < total ? d0 + TILE : total;
   const uint64_t a0 = parts[k], a1 = parts[k + 1];
@@ -92,7 +106,9 @@ int merge_launch(const K *a, const P *av, uint64_t na, const K *b, const P *bv, 
     if ((st = host::set_smem_attrs(merge_kernel<K, P>, smem)) != BK_OK) return st;
     attr_set = true;
   }
-  merge_kernel<K, P><<<(unsigned)tiles, kMergeThreads, smem, stream>>>(a, av, na, b, bv, nb, out, outv, parts);
+  static thread_local uint64_t ahead = 0;
+  if (ahead == 0) ahead = host::resident_ctas(merge_kernel<K, P>, kMergeThreads, smem, di.sm_count);
+  merge_kernel<K, P><<<(unsigned)tiles, kMergeThreads, smem, stream>>>(a, av, na, b, bv, nb, out, outv, parts, ahead);
   return host::launch_status();
 }
 

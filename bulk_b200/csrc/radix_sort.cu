@@ -165,12 +165,27 @@ struct RsBatch {
 // read warp-striped (element w*512 + j*32 + lane: coalesced) and counted with
 // shared-memory atomics into one histogram per warp; a warp whose 32 keys
 // share one digit adds 32 with one atomic (constant high digits are common).
+// Tile g's keys (and payloads) of this pass into L2, for the CTA that will
+// start about when every CTA now resident has finished.
+template <typename K, typename P, typename Src>
+__device__ __forceinline__ void rs_prefetch_tile(const Src &src, unsigned int g, int pass, bool payload) {
+  if (g >= gridDim.x) return;
+  const RsTile<K, P> f = src.tile(g);
+  const uint64_t base = (uint64_t)f.local * kRsTile;
+  const uint64_t cnt = (f.n - base) < (uint64_t)kRsTile ? (f.n - base) : (uint64_t)kRsTile;
+  prefetch_l2_range(((pass & 1) ? f.tk : f.keys) + base, cnt * sizeof(K));
+  if constexpr (has_payload<P>()) {
+    if (payload) prefetch_l2_range(((pass & 1) ? f.tv : f.vals) + base, cnt * sizeof(P));
+  }
+}
+
 template <typename K, typename P, typename Src>
 __global__ void __launch_bounds__(kRsThreads) rs_upsweep_kernel(const __grid_constant__ Src src, int pass,
-                                                                unsigned int *counts) {
+                                                                unsigned int *counts, unsigned int ahead) {
   __shared__ unsigned int s_wcnt[kRsWarps][kRsBins];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int shift = 8 * pass;
+  if (tid == 0) rs_prefetch_tile<K, P>(src, blockIdx.x + ahead, pass, false);
   const RsTile<K, P> tl = src.tile(blockIdx.x);
   const K *in_k = (pass & 1) ? tl.tk : tl.keys;
   const uint64_t tbase = (uint64_t)tl.local * kRsTile;
@@ -215,7 +230,7 @@ constexpr int rs_down_min_blocks() {
 template <typename K, typename P, typename Src, int V, int TH>
 __global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downsweep_kernel(
     const __grid_constant__ Src src, int pass, const unsigned int *scanned, const WsHeader *scan_hdr,
-    WsHeader *hdr) {
+    WsHeader *hdr, unsigned int ahead) {
   constexpr int ITEMS = kRsTile / TH, WARPS = TH / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   K *sk = reinterpret_cast<K *>(smem);  // the tile in digit order
@@ -230,6 +245,7 @@ __global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downswe
     return;
   }
   const int shift = 8 * pass;
+  if (tid == 0) rs_prefetch_tile<K, P>(src, blockIdx.x + ahead, pass, true);
   const RsTile<K, P> tl = src.tile(blockIdx.x);
   const K *in_k = (pass & 1) ? tl.tk : tl.keys;
   const P *in_v = (pass & 1) ? tl.tv : tl.vals;
@@ -397,21 +413,27 @@ int radix_sort_run(const Src &src, const RsLayout<K, P> &L, char *ws, cudaStream
   auto *hdr = reinterpret_cast<WsHeader *>(ws);
   const auto *scan_hdr = reinterpret_cast<const WsHeader *>(scan_ws);
   static thread_local bool attr_set = false;
+  static thread_local unsigned int up_ahead = 0, down_ahead = 0;
   if (!attr_set) {
     if ((st = host::set_smem_attrs(rs_downsweep_kernel<K, P, Src, kDownV, kDownTh>, rs_smem_bytes<K, P>())) != BK_OK)
       return st;
+    host::DeviceInfo di;
+    if ((st = host::device_info(&di)) != BK_OK) return st;
+    up_ahead = (unsigned)host::resident_ctas(rs_upsweep_kernel<K, P, Src>, kRsThreads, 0, di.sm_count);
+    down_ahead = (unsigned)host::resident_ctas(rs_downsweep_kernel<K, P, Src, kDownV, kDownTh>, kDownTh,
+                                               rs_smem_bytes<K, P>(), di.sm_count);
     attr_set = true;
   }
   // the scan's workspace must start zeroed, like any workspace
   if ((st = host::from_cuda(cudaMemsetAsync(scan_ws, 0, kHeaderBytes, stream))) != BK_OK) return st;
   for (int p = 0; p < rs_passes<K>(); ++p) {
-    rs_upsweep_kernel<K, P, Src><<<(unsigned)L.tiles, kRsThreads, 0, stream>>>(src, p, counts);
+    rs_upsweep_kernel<K, P, Src><<<(unsigned)L.tiles, kRsThreads, 0, stream>>>(src, p, counts, up_ahead);
     if ((st = host::launch_status()) != BK_OK) return st;
     st = bk_inclusive_scan_sum_u32(counts, L.tiles * kRsBins, 0u, counts, scan_ws, L.scan_ws_bytes,
                                    (bk_stream_t)stream);
     if (st != BK_OK) return st;
     rs_downsweep_kernel<K, P, Src, kDownV, kDownTh><<<(unsigned)L.tiles, kDownTh, rs_smem_bytes<K, P>(), stream>>>(
-        src, p, counts, scan_hdr, hdr);
+        src, p, counts, scan_hdr, hdr, down_ahead);
     if ((st = host::launch_status()) != BK_OK) return st;
   }
   return BK_OK;
