@@ -53,6 +53,16 @@ def test_rbk_item_layout(kv):
     assert ctypes.sizeof(rbk_item_type(*kv)) == 48
 
 
+@pytest.mark.parametrize("algo,kv", [("reduce_by_key", ("i32", "f32")), ("reduce_by_key", ("i64", "f64")),
+                                     ("inclusive_scan", ("f32", None)), ("inclusive_scan", ("u64", None))])
+def test_batch_of_one_needs_what_one_call_needs(algo, kv):
+    for n in (1, 4096, 100003, 1 << 22):
+        assert batch_workspace_bytes(algo, kv[0], kv[1], [n]) == bulk_b200.workspace_bytes(algo, kv[0], kv[1], n)
+    # more arrays never need less
+    assert batch_workspace_bytes(algo, kv[0], kv[1], [5000, 7000]) >= batch_workspace_bytes(algo, kv[0], kv[1],
+                                                                                            [7000])
+
+
 def test_sort_item_layout_and_workspace():
     assert ctypes.sizeof(sort_item_type("u32", "u32")) == 24
     # a one-array batch needs what the single-array call needs; more arrays need more
