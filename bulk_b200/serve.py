@@ -56,8 +56,11 @@ class DevicePool:
 
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
-        if h:
-            lib.bk_pool_destroy(h)
+        if h and lib is not None:
+            try:
+                lib.bk_pool_destroy(h)
+            except (AttributeError, TypeError):  # interpreter shutdown
+                pass
 
     def alloc(self, nbytes: int) -> int | None:
         off = ctypes.c_uint64()
