@@ -266,6 +266,12 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       if (!tx) mbar_arrive(&s_full[bn]);
       ++armed[bn];
       next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
+      // tiles are ticketed about in order, gridDim.x per iteration: ask L2
+      // now for the one some CTA will load an iteration from now
+      if (tn != NONE && tn + gridDim.x < num_tiles) {
+        const ScanTile<T> f = src.tile(tn + gridDim.x);
+        prefetch_l2_range(f.in, (uint64_t)f.count * sizeof(T));
+      }
       // once the compute warps are done with buffer bt (phase 1 of t, or
       // just its empty phase), re-read t_{i-1} from L2 into it
       if (!mbar_wait_or_abort(&s_p1[bt], p1par[bt], spin_limit_ns, &s_abort)) {

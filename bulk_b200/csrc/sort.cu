@@ -272,11 +272,15 @@ __global__ void sort_partition_kernel(const __grid_constant__ Src src, uint64_t 
   m.parts[m.local] = merge_path<K, uint64_t>(m.src_k + p0, a_end - p0, m.src_k + a_end, b_end - a_end, d - p0);
 }
 
-template <typename K, typename P, typename Src>
-__global__ void __launch_bounds__(kMpThreads, 4) sort_merge_kernel(const __grid_constant__ Src src) {
+// A merge-pass tile's inputs: elements [a_lo, a_lo + la) and [b_lo, b_lo + lb)
+// of the source array, and its first output element.
+struct MpRanges {
+  uint64_t a_lo, b_lo, out;
+  int la, lb;
+};
+template <typename K, typename P>
+__device__ __forceinline__ MpRanges mp_ranges(const MpTile<K, P> &m) {
   constexpr uint64_t T = SortCfg<K>::MP_TILE;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const MpTile<K, P> m = src.tile(blockIdx.x);
   const uint64_t t = m.local, n = m.n, w = m.w;
   const uint64_t d = t * T;
   const uint64_t p0 = d / (2 * w) * (2 * w);
@@ -289,12 +293,33 @@ __global__ void __launch_bounds__(kMpThreads, 4) sort_merge_kernel(const __grid_
   // the next tile's split belongs to this pair only if it starts inside it
   const uint64_t a1 = (t + 1 < m.num_tiles && d + T < b_end) ? m.parts[t + 1] : la_all;
   const uint64_t b0 = diag0 - a0, b1 = diag1 - a1;
+  return MpRanges{p0 + a0, a_end + b0, d, (int)(a1 - a0), (int)(b1 - b0)};
+}
+
+// One merge-pass tile per CTA.  Thread 0 first asks L2 for the inputs of
+// global tile blockIdx.x + ahead (the CTA that will start about when every CTA
+// now resident has finished).
+template <typename K, typename P, typename Src>
+__global__ void __launch_bounds__(kMpThreads, 4) sort_merge_kernel(const __grid_constant__ Src src, uint64_t ahead) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (threadIdx.x == 0 && blockIdx.x + ahead < gridDim.x) {
+    const MpTile<K, P> f = src.tile(blockIdx.x + ahead);
+    const MpRanges r = mp_ranges<K, P>(f);
+    prefetch_l2_range(f.src_k + r.a_lo, (uint64_t)r.la * sizeof(K));
+    prefetch_l2_range(f.src_k + r.b_lo, (uint64_t)r.lb * sizeof(K));
+    if constexpr (has_payload<P>()) {
+      prefetch_l2_range(f.src_v + r.a_lo, (uint64_t)r.la * sizeof(P));
+      prefetch_l2_range(f.src_v + r.b_lo, (uint64_t)r.lb * sizeof(P));
+    }
+  }
+  const MpTile<K, P> m = src.tile(blockIdx.x);
+  const MpRanges r = mp_ranges<K, P>(m);
   const K *sk = m.src_k;
   const P *sv = m.src_v;
   merge_tile<kMpThreads, SortCfg<K>::MP_ITEMS, K, P>(
-      sk + p0 + a0, has_payload<P>() ? sv + p0 + a0 : nullptr, (int)(a1 - a0), sk + a_end + b0,
-      has_payload<P>() ? sv + a_end + b0 : nullptr, (int)(b1 - b0), m.dst_k + d,
-      has_payload<P>() ? m.dst_v + d : nullptr, smem);
+      sk + r.a_lo, has_payload<P>() ? sv + r.a_lo : nullptr, r.la, sk + r.b_lo,
+      has_payload<P>() ? sv + r.b_lo : nullptr, r.lb, m.dst_k + r.out, has_payload<P>() ? m.dst_v + r.out : nullptr,
+      smem);
 }
 
 template <typename K, typename P>
@@ -329,15 +354,22 @@ int sort_passes(uint64_t n) {
   return passes;
 }
 
+// Sets the kernels' shared-memory attributes once and returns (in *ahead)
+// how many merge-pass CTAs are resident at once.
 template <typename K, typename P, typename BsSrc, typename MpSrc>
-int sort_set_attrs() {
+int sort_set_attrs(uint64_t *ahead) {
   static thread_local bool attr_set = false;
+  static thread_local uint64_t mp_resident = 0;
   if (!attr_set) {
     int st;
     if ((st = set_smem(block_sort_kernel<K, P, BsSrc>, bs_smem_bytes<K, P>())) != BK_OK) return st;
     if ((st = set_smem(sort_merge_kernel<K, P, MpSrc>, mp_smem_bytes<K, P>())) != BK_OK) return st;
+    host::DeviceInfo di;
+    if ((st = host::device_info(&di)) != BK_OK) return st;
+    mp_resident = host::resident_ctas(sort_merge_kernel<K, P, MpSrc>, kMpThreads, mp_smem_bytes<K, P>(), di.sm_count);
     attr_set = true;
   }
+  *ahead = mp_resident;
   return BK_OK;
 }
 
@@ -372,7 +404,8 @@ int sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaS
   ws += align_up(n * (size_t)payload_bytes<P>(), 256);
   uint64_t *parts = reinterpret_cast<uint64_t *>(ws);
   const int passes = sort_passes<K>(n);
-  if ((st = sort_set_attrs<K, P, BsOne<K, P>, MpOne<K, P>>()) != BK_OK) return st;
+  uint64_t ahead = 0;
+  if ((st = sort_set_attrs<K, P, BsOne<K, P>, MpOne<K, P>>(&ahead)) != BK_OK) return st;
   // an odd number of passes starts in the temporaries so the last lands in place
   K *ck = (passes & 1) ? tk : keys;
   P *cv = (passes & 1) ? tv : vals;
@@ -385,7 +418,7 @@ int sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes, cudaS
     const MpOne<K, P> src{ck, cv, nk, nv, n, w, parts, mp_tiles};
     sort_partition_kernel<K, P, MpOne<K, P>><<<(unsigned)((mp_tiles + 255) / 256), 256, 0, stream>>>(src, mp_tiles);
     if ((st = host::launch_status()) != BK_OK) return st;
-    sort_merge_kernel<K, P, MpOne<K, P>><<<(unsigned)mp_tiles, kMpThreads, mp_smem_bytes<K, P>(), stream>>>(src);
+    sort_merge_kernel<K, P, MpOne<K, P>><<<(unsigned)mp_tiles, kMpThreads, mp_smem_bytes<K, P>(), stream>>>(src, ahead);
     if ((st = host::launch_status()) != BK_OK) return st;
     ck = nk;
     cv = nv;
@@ -503,7 +536,8 @@ int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, s
   if (na == 0) return BK_OK;
   bs.start[bs.count] = (uint32_t)bs_total;
   if (bs_total >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
-  if ((st = sort_set_attrs<K, P, BsBatch<K, P>, MpBatch<K, P>>()) != BK_OK) return st;
+  uint64_t ahead = 0;
+  if ((st = sort_set_attrs<K, P, BsBatch<K, P>, MpBatch<K, P>>(&ahead)) != BK_OK) return st;
   block_sort_kernel<K, P, BsBatch<K, P>><<<(unsigned)bs_total, kBsThreads, bs_smem_bytes<K, P>(), stream>>>(bs);
   if ((st = host::launch_status()) != BK_OK) return st;
   // pass p merges runs of width BS_TILE << p for every array with more than p passes
@@ -532,7 +566,7 @@ int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, s
     if (mp_total >= 0x7fffffffull) return BK_ERR_TOO_LARGE;
     sort_partition_kernel<K, P, MpBatch<K, P>><<<(unsigned)((mp_total + 255) / 256), 256, 0, stream>>>(mp, mp_total);
     if ((st = host::launch_status()) != BK_OK) return st;
-    sort_merge_kernel<K, P, MpBatch<K, P>><<<(unsigned)mp_total, kMpThreads, mp_smem_bytes<K, P>(), stream>>>(mp);
+    sort_merge_kernel<K, P, MpBatch<K, P>><<<(unsigned)mp_total, kMpThreads, mp_smem_bytes<K, P>(), stream>>>(mp, ahead);
     if ((st = host::launch_status()) != BK_OK) return st;
   }
   return BK_OK;
