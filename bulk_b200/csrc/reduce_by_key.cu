@@ -294,7 +294,8 @@ struct LaneRun {
 // Loads a lane's M consecutive keys and values of a staged tile (element
 // index of its first: e0 = (warp * 32 + lane) * M); elements past the tile's
 // end read as key K() and value 0.
-template <typename K, typename V>
+// FULL: the tile holds TILE elements, so every lane's are all inside it.
+template <typename K, typename V, bool FULL>
 __device__ __forceinline__ void rbk_load_lane(const unsigned char *buf, uint32_t count, int warp, int lane,
                                               LaneRun<K, V, RbkCfg<K, V>::M> &lr) {
   using C = RbkCfg<K, V>;
@@ -302,9 +303,9 @@ __device__ __forceinline__ void rbk_load_lane(const unsigned char *buf, uint32_t
   const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
   load_lane_rotated<M * sizeof(K)>(lr.key, buf, e0 * (uint32_t)sizeof(K), lane);
   load_lane_rotated<M * sizeof(V)>(lr.val, buf + C::KEY_BYTES, e0 * (uint32_t)sizeof(V), lane);
-  const int nvalid = (int)min(max((int)count - (int)e0, 0), M);
+  const int nvalid = FULL ? M : (int)min(max((int)count - (int)e0, 0), M);
   lr.nvalid = nvalid;
-  if (nvalid < M) {
+  if (!FULL && nvalid < M) {
 #pragma unroll
     for (int j = 0; j < M; ++j)
       if (j >= nvalid) {
@@ -321,7 +322,7 @@ __device__ __forceinline__ void rbk_load_lane(const unsigned char *buf, uint32_t
 // reads the key before the warp's range from shared memory, or the halo
 // hb[0][KC-1] before the tile.  first_tile: the tile starts the input;
 // last_tile: it ends it.
-template <typename K, typename V>
+template <typename K, typename V, bool FULL>
 __device__ __forceinline__ void rbk_flags(const unsigned char *buf, const K (*hb)[16 / sizeof(K)], uint32_t count,
                                           bool first_tile, bool last_tile, int warp, int lane,
                                           LaneRun<K, V, RbkCfg<K, V>::M> &lr) {
@@ -330,7 +331,7 @@ __device__ __forceinline__ void rbk_flags(const unsigned char *buf, const K (*hb
   constexpr int KC = 16 / sizeof(K);
   const K *sk = reinterpret_cast<const K *>(buf);
   const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;
-  const int nvalid = lr.nvalid;
+  const int nvalid = FULL ? M : lr.nvalid;
   K prev = shfl_up(lr.key[M - 1], 1);
   K next = shfl_down_any(lr.key[0], 1);
   if (lane == 0) prev = e0 == 0 ? hb[0][KC - 1] : sk[e0 - 1];
@@ -595,8 +596,13 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
       const RbkTile<K, V> tl = src.tile(t);
       const uint32_t count = tl.count();
       LaneRun<K, V, M> lr;
-      rbk_load_lane<K, V>(buf(bt), count, warp, lane, lr);
-      rbk_flags<K, V>(buf(bt), s_halo[bt], count, tl.first(), tl.last(), warp, lane, lr);
+      if (count == (uint32_t)TILE) {  // every tile but an array's last: no bounds checks
+        rbk_load_lane<K, V, true>(buf(bt), count, warp, lane, lr);
+        rbk_flags<K, V, true>(buf(bt), s_halo[bt], count, tl.first(), tl.last(), warp, lane, lr);
+      } else {
+        rbk_load_lane<K, V, false>(buf(bt), count, warp, lane, lr);
+        rbk_flags<K, V, false>(buf(bt), s_halo[bt], count, tl.first(), tl.last(), warp, lane, lr);
+      }
       V *marks = cta_ring + (size_t)(it % 3) * TILE + (warp * 32 + lane) * M;
       const P incl = warp_inclusive_scan(lane_fold_mark(lr, marks), op, lane);
       fence_proxy_async_global();  // the marks are read back by a TMA copy
