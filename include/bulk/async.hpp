@@ -9,9 +9,16 @@
 // future, anything else into the legacy default stream.  The launch layer is
 // this library's own (SURVEY.md's rewrite of cuda_launcher / choose_sizes):
 //   parallel_group<agent<G>> of n agents   grid-stride loop, 256-thread CTAs,
-//                                          at most 8 CTAs per SM
+//                                          at most as many CTAs as are resident
+//                                          at once
 //   concurrent_group<agent<G>, S>          one CTA of S threads
-//   parallel_group<concurrent_group<...>>  n CTAs of S threads
+//   parallel_group<concurrent_group<...>>  n CTAs of S threads; an unspecified
+//                                          n is the number resident at once
+// "Resident at once" is the CUDA runtime's occupancy model of the kernel as
+// compiled for this functor (its registers, static and dynamic shared
+// memory) times the SM count, so grids follow each kernel instead of a fixed
+// table (the reference sizes them by a pre-Maxwell occupancy calculator,
+// bulk/detail/cuda_launcher/cuda_launch_config.hpp:240-379).
 // Concurrent groups get a dynamic shared-memory heap (bulk/malloc.hpp): the
 // requested heap size, or by default the share of an SM's shared memory that
 // keeps every group that fits by threads resident (opted in above 48 KB).
@@ -146,6 +153,18 @@ inline void opt_in_smem(Kernel k, unsigned int bytes) {
 
 inline int default_group_size(int requested) { return requested == use_default ? 256 : requested; }
 
+// CTAs of kernel k one SM holds at once with `threads` threads and `smem`
+// bytes of dynamic shared memory (at least 1).
+template <typename Kernel>
+inline int resident_per_sm(Kernel k, int threads, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess || per_sm < 1) {
+    (void)cudaGetLastError();  // a failed query leaves no sticky error behind
+    per_sm = 1;
+  }
+  return per_sm;
+}
+
 // ---- launch into a stream ----------------------------------------------------
 template <typename Agent, std::size_t N, typename F, typename... Args>
 void launch(const parallel_group<Agent, N> &g, cudaStream_t s, F f, Args... args) {
@@ -153,22 +172,20 @@ void launch(const parallel_group<Agent, N> &g, cudaStream_t s, F f, Args... args
     // a grid of concurrent groups (one CTA each)
     const Agent &proto_in = g.this_exec;
     const int size = default_group_size(proto_in.size());
-    int num_groups = g.size();
-    if (num_groups == use_default) {
-      const device_props p = device_properties();
-      num_groups = p.sm_count * std::max(1, p.max_threads_per_sm / size);
-    }
     const unsigned int heap = choose_heap(size, proto_in.heap_size());
     Agent proto = make_group_size(proto_in, size, (int)heap);
     auto k = async_grid_of_groups<Agent, F, Args...>;
     opt_in_smem(k, heap);
+    int num_groups = g.size();
+    if (num_groups == use_default) num_groups = device_properties().sm_count * resident_per_sm(k, size, heap);
     if (num_groups > 0) k<<<num_groups, size, heap, s>>>(num_groups, proto, heap, f, args...);
   } else {
     const int n = g.size();
-    const device_props p = device_properties();
     const int threads = 256;
-    const int blocks = std::max(1, std::min((n + threads - 1) / threads, p.sm_count * 8));
-    if (n > 0) async_parallel_agents<Agent, F, Args...><<<blocks, threads, 0, s>>>(n, f, args...);
+    auto k = async_parallel_agents<Agent, F, Args...>;
+    const int resident = device_properties().sm_count * resident_per_sm(k, threads, 0);
+    const int blocks = std::max(1, std::min((n + threads - 1) / threads, resident));
+    if (n > 0) k<<<blocks, threads, 0, s>>>(n, f, args...);
   }
   throw_on_error(cudaGetLastError(), "bulk::async: launch");
 }
@@ -208,17 +225,21 @@ future<void> async(async_launch<ExecutionGroup> policy, F f, Args... args) {
   return detail::future_core_access::create(s, owns);
 }
 
-// The group size and count bulk::async would choose for a grid of
-// concurrent groups (replaces the reference's occupancy-based choose_sizes,
-// bulk/choose_sizes.hpp:29-75): unspecified sizes become 256 threads per
-// group and as many groups as fill every SM by thread count.
+// The group count and size bulk::async would choose for a grid of
+// concurrent groups running f(args...) (replaces the reference's
+// occupancy-based choose_sizes, bulk/choose_sizes.hpp:29-75): an unspecified
+// size becomes 256 threads per group, an unspecified count the number of
+// such groups resident at once under the runtime's occupancy model of this
+// kernel with its heap.
 template <typename F, typename... Args>
 std::pair<int, int> choose_sizes(parallel_group<concurrent_group<>> g, F, Args...) {
   const int size = detail::default_group_size(g.this_exec.size());
   int num = g.size();
   if (num == use_default) {
-    const detail::device_props p = detail::device_properties();
-    num = p.sm_count * std::max(1, p.max_threads_per_sm / size);
+    const unsigned int heap = detail::choose_heap(size, g.this_exec.heap_size());
+    auto k = detail::async_grid_of_groups<concurrent_group<>, F, Args...>;
+    detail::opt_in_smem(k, heap);
+    num = detail::device_properties().sm_count * detail::resident_per_sm(k, size, heap);
   }
   return std::make_pair(num, size);
 }

@@ -191,6 +191,13 @@ struct segment_scan {  // one group per segment
   }
 };
 
+struct count_groups {  // one mark per group, written by its first agent
+  __device__ void operator()(bulk::concurrent_group<> &g, int *marks, int cap) {
+    if (g.this_exec.index() == 0 && g.index() < cap) atomicAdd(&marks[g.index()], 1);
+    if (g.this_exec.index() == 0 && g.index() >= cap) atomicAdd(&marks[cap], 1);
+  }
+};
+
 static void driver_programs() {
   {
     dvec<int> out(32);
@@ -252,6 +259,23 @@ static void driver_programs() {
     got.resize(4);
     check("futures par(stream) -> par(future) order", got, std::vector<int>{3, 1, 2, 3});
     CUDA_OK(cudaStreamDestroy(s1));
+  }
+  {
+    // an unspecified grid: as many 256-thread groups as the occupancy model
+    // says are resident at once (a whole number per SM), each launched once
+    int sms = 0;
+    CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
+    const int cap = 1 << 16;
+    dvec<int> marks(cap + 1);
+    CUDA_OK(cudaMemset(marks.p, 0, sizeof(int) * (cap + 1)));
+    stage("count_groups");
+    const std::pair<int, int> sz = bulk::choose_sizes(bulk::grid(), count_groups(), bulk::root.this_exec, marks.p, cap);
+    check_true("choose_sizes default grid: 256 threads, whole groups per SM",
+               sz.second == 256 && sz.first >= sms && sz.first % sms == 0 && sz.first <= 8 * sms);
+    bulk::async(bulk::grid(), count_groups(), bulk::root.this_exec, marks.p, cap).wait();
+    std::vector<int> want(cap + 1, 0);
+    for (int i = 0; i < sz.first && i < cap; ++i) want[i] = 1;
+    check("default grid launches the chosen number of groups", marks.get(), want);
   }
   {
     const int groups = 300, seg = 1000;

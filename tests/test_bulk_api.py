@@ -60,7 +60,8 @@ def test_api_program_runs(api_binary):
     assert lines and lines[-1].startswith("PASSED")
     # every family of the interface was exercised
     text = r.stdout
-    for name in ["hello_world", "saxpy", "sum con(512)", "futures", "grid<128,4>", "group reduce n=",
+    for name in ["hello_world", "saxpy", "sum con(512)", "futures", "choose_sizes default grid",
+                 "default grid launches", "grid<128,4>", "group reduce n=",
                  "non-commutative", "group inclusive_scan", "group exclusive_scan", "group copy_n", "gather",
                  "scatter_if", "for_each_n", "adjacent_difference", "strided_iterator", "group merge na=",
                  "merge_by_key", "inplace_merge", "stable_sort_by_key", "group stable_sort n=",
