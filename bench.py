@@ -11,7 +11,8 @@ value  = algorithmic bytes per step (reduce N*s, scan 2*N*s) / device time,
          GPU: replicas, weak scaling).
 e2e    = the same through the C-ABI with host buffers: pinned-host -> device
          copies of the step's inputs and device -> host copies of every result
-         inside the timed region.
+         inside the timed region (one stream per array, so copies in the two
+         directions overlap).
 ops    = per-op GB/s: the headline's six calls, and the other benchmark
          configurations (merge_by_key 2 x 2^26 f32/u32, stable sort_by_key
          2^26 u32/u64 keys with u32 payload, reduce_by_key 2^27 i32 keys with
@@ -290,11 +291,16 @@ def headline(args, device, rank, world):
 
 
 def e2e(args, device, xs):
-    """Same workload through the public API with host buffers (pinned), copies timed."""
+    """Same workload through the public API with host buffers (pinned), copies timed.
+
+    Each dtype's array goes through its own stream (copy in, reduce, scan,
+    copy out), so one array's copy to the host overlaps the next one's copy to
+    the device: the two directions use separate copy engines."""
     import torch
 
     import bulk_b200
     stream = torch.cuda.current_stream(device)
+    streams = {k: torch.cuda.Stream(device) for k, _ in DTYPES}
     h_in = {k: v.cpu().pin_memory() for k, v in xs.items()}
     h_scan = {k: torch.empty_like(v, device="cpu").pin_memory() for k, v in xs.items()}
     h_red = {k: torch.empty(1, dtype=v.dtype).pin_memory() for k, v in xs.items()}
@@ -306,11 +312,13 @@ def e2e(args, device, xs):
 
     def step():
         for k, _ in DTYPES:
-            d_in[k].copy_(h_in[k], non_blocking=True)
-            bulk_b200.reduce(d_in[k], 0, out=d_red[k])
-            bulk_b200.inclusive_scan(d_in[k], 0, out=d_out[k])
-            h_red[k].copy_(d_red[k], non_blocking=True)
-            h_scan[k].copy_(d_out[k], non_blocking=True)
+            s = streams[k]
+            with torch.cuda.stream(s):
+                d_in[k].copy_(h_in[k], non_blocking=True)
+                bulk_b200.reduce(d_in[k], 0, out=d_red[k], stream=s)
+                bulk_b200.inclusive_scan(d_in[k], 0, out=d_out[k], stream=s)
+                h_red[k].copy_(d_red[k], non_blocking=True)
+                h_scan[k].copy_(d_out[k], non_blocking=True)
 
     steps = max(1, min(args.steps, args.e2e_steps))
     for _ in range(min(args.warmup, 3)):
@@ -318,8 +326,12 @@ def e2e(args, device, xs):
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
+    for s in streams.values():
+        s.wait_event(a)
     for _ in range(steps):
         step()
+    for s in streams.values():
+        stream.wait_stream(s)
     b.record(stream)
     torch.cuda.synchronize()
     return a.elapsed_time(b) / steps, h2d, d2h, steps
