@@ -189,6 +189,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
   __shared__ __align__(8) uint64_t s_qbar[Q];
   __shared__ unsigned int s_ticket[NB];  // ticket of the tile prefetched into buffer b
   __shared__ T s_wtot[4][kScanWarps];    // per-warp totals of t_i, by iteration mod 4
+  __shared__ T s_wexcl[4][kScanWarps];   // the warps before each warp, folded (thread 0)
   __shared__ unsigned int s_q_tile[Q];   // look-back queue: entry j = t_j
   __shared__ T s_q_agg[Q];
   __shared__ T s_q_prefix[Q];
@@ -400,20 +401,33 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       const uint32_t count = tl.count;
       const T *bT = buf(bt);
       T a = Op::identity();
+      if (tl.tma && count == (uint32_t)C::TILE) {
+        // a full tile in shared memory: no element is past its end
 #pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
-        T x[V];
-        if (tl.tma) {
+        for (int k = 0; k < R; ++k) {
+          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+          T x[V];
           const uint4 c = reinterpret_cast<const uint4 *>(bT)[elem / V];
           memcpy(&x[0], &c, 16);
-        } else {
 #pragma unroll
-          for (int j = 0; j < V; ++j) x[j] = (elem + j < count) ? tl.in[elem + j] : Op::identity();
+          for (int j = 0; j < V; ++j) a = op(a, x[j]);
         }
+      } else {
 #pragma unroll
-        for (int j = 0; j < V; ++j)
-          if (elem + j < count) a = op(a, x[j]);
+        for (int k = 0; k < R; ++k) {
+          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+          T x[V];
+          if (tl.tma) {
+            const uint4 c = reinterpret_cast<const uint4 *>(bT)[elem / V];
+            memcpy(&x[0], &c, 16);
+          } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j) x[j] = (elem + j < count) ? tl.in[elem + j] : Op::identity();
+          }
+#pragma unroll
+          for (int j = 0; j < V; ++j)
+            if (elem + j < count) a = op(a, x[j]);
+        }
       }
       a = warp_reduce(a, op);
       if (lane == 0) s_wtot[it & 3][warp] = a;
@@ -430,8 +444,12 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       T agg = Op::identity();
       if (t != NONE) {
         agg = s_wtot[it & 3][0];
+        s_wexcl[it & 3][0] = Op::identity();
 #pragma unroll
-        for (int i = 1; i < kScanWarps; ++i) agg = op(agg, s_wtot[it & 3][i]);
+        for (int i = 1; i < kScanWarps; ++i) {
+          s_wexcl[it & 3][i] = agg;
+          agg = op(agg, s_wtot[it & 3][i]);
+        }
         if ((long long)t != skip_publish_tile) {
           const ScanTile<T> tl = src.tile(t);
           if (tl.first) st.publish(t, kStPrefix, op(tl.init, agg));
@@ -456,8 +474,8 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       const uint32_t count = tl.count;
       T *const bP = buf(bp);
       const unsigned int e = (unsigned int)it - 2u;
-      T before = s_q_prefix[e % Q];  // everything before this warp's first element
-      for (int i = 0; i < warp; ++i) before = op(before, s_wtot[(it + 2) & 3][i]);
+      // everything before this warp's first element
+      T before = warp == 0 ? s_q_prefix[e % Q] : op(s_q_prefix[e % Q], s_wexcl[(it + 2) & 3][warp]);
       T y[R][V], incl[R];
 #pragma unroll
       for (int k = 0; k < R; ++k) {
