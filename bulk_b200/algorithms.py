@@ -54,9 +54,12 @@ def _ptr(t: torch.Tensor | None) -> int | None:
     return None if t is None else t.data_ptr()
 
 
+def _stream_obj(stream: torch.cuda.Stream | None, device: torch.device) -> torch.cuda.Stream:
+    return stream if stream is not None else torch.cuda.current_stream(device)
+
+
 def _stream_handle(stream: torch.cuda.Stream | None, device: torch.device) -> int:
-    s = stream if stream is not None else torch.cuda.current_stream(device)
-    return s.cuda_stream
+    return _stream_obj(stream, device).cuda_stream
 
 
 def _require_cuda(*ts: torch.Tensor) -> torch.device:
@@ -80,19 +83,25 @@ class _WorkspacePool:
 
     The library leaves every workspace's counters zeroed after each call, so a
     workspace is reused across calls on the same stream without re-clearing.
+    A workspace is allocated and zero-filled on the stream that uses it, so the
+    fill is ordered before the library's kernels there; when it grows, the old
+    buffer goes back to torch's caching allocator as a block of that stream,
+    which hands it out again only in that stream's order, after the kernels
+    already queued on it.
     """
 
     def __init__(self):
         self._lock = threading.Lock()
         self._ws: dict[tuple[int, int], torch.Tensor] = {}
 
-    def get(self, nbytes: int, device: torch.device, stream: int) -> tuple[int, int]:
-        key = (device.index if device.index is not None else torch.cuda.current_device(), stream)
+    def get(self, nbytes: int, device: torch.device, stream: torch.cuda.Stream) -> tuple[int, int]:
+        key = (device.index if device.index is not None else torch.cuda.current_device(), stream.cuda_stream)
         with self._lock:
             t = self._ws.get(key)
             if t is None or t.numel() < nbytes:
                 size = max(nbytes, 1 << 16, 0 if t is None else 2 * t.numel())
-                t = torch.zeros(size, dtype=torch.uint8, device=device)
+                with torch.cuda.stream(stream):
+                    t = torch.zeros(size, dtype=torch.uint8, device=device)
                 self._ws[key] = t
             return t.data_ptr(), t.numel()
 
@@ -126,7 +135,7 @@ def debug_set_fault(skip_publish_tile: int = -1, spin_limit_ns: int = 0) -> None
     check(lib.bk_debug_set_fault(skip_publish_tile, spin_limit_ns), "bk_debug_set_fault")
 
 
-def _ws(algo, key, value, n, device, stream):
+def _ws(algo, key, value, n, device, stream: torch.cuda.Stream):
     need = workspace_bytes(algo, key, value, n)
     if need == 0 and algo not in ("reduce",):
         return None, 0
@@ -141,10 +150,12 @@ def reduce(x: torch.Tensor, init=0, op: str = "sum", out: torch.Tensor | None = 
     tag = dtype_tag(x.dtype)
     if out is None:
         out = torch.empty(1, dtype=x.dtype, device=dev)
-    s = _stream_handle(stream, dev)
-    ws, wsb = _ws("reduce", tag, None, x.numel(), dev, s)
-    fn = getattr(lib, f"bk_reduce_{op}_{tag}")
-    check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
+    with torch.cuda.device(dev):
+        so = _stream_obj(stream, dev)
+        s = so.cuda_stream
+        ws, wsb = _ws("reduce", tag, None, x.numel(), dev, so)
+        fn = getattr(lib, f"bk_reduce_{op}_{tag}")
+        check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
     return out
 
 
@@ -155,10 +166,12 @@ def inclusive_scan(x: torch.Tensor, init=0, op: str = "sum", out: torch.Tensor |
     tag = dtype_tag(x.dtype)
     if out is None:
         out = torch.empty_like(x)
-    s = _stream_handle(stream, dev)
-    ws, wsb = _ws("inclusive_scan", tag, None, x.numel(), dev, s)
-    fn = getattr(lib, f"bk_inclusive_scan_{op}_{tag}")
-    check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
+    with torch.cuda.device(dev):
+        so = _stream_obj(stream, dev)
+        s = so.cuda_stream
+        ws, wsb = _ws("inclusive_scan", tag, None, x.numel(), dev, so)
+        fn = getattr(lib, f"bk_inclusive_scan_{op}_{tag}")
+        check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
     return out
 
 
@@ -183,19 +196,21 @@ def merge(a: torch.Tensor, b: torch.Tensor, a_vals: torch.Tensor | None = None, 
     n = a.numel() + b.numel()
     if out is None:
         out = torch.empty(n, dtype=a.dtype, device=dev)
-    s = _stream_handle(stream, dev)
-    ws, wsb = _ws("merge", tag, _payload_tag(a_vals), n, dev, s)
-    if a_vals is None:
-        fn = getattr(lib, f"bk_merge_{tag}")
-        check(fn(_ptr(a), a.numel(), _ptr(b), b.numel(), _ptr(out), ws, wsb, s), fn.__name__)
-        return out
-    if b_vals is None or a_vals.element_size() != b_vals.element_size():
+    if a_vals is not None and (b_vals is None or a_vals.element_size() != b_vals.element_size()):
         raise TypeError("a_vals and b_vals must both be given, with the same element size")
-    if out_vals is None:
+    if a_vals is not None and out_vals is None:
         out_vals = torch.empty(n, dtype=a_vals.dtype, device=dev)
-    fn = getattr(lib, f"bk_merge_by_key_{tag}_{_payload_tag(a_vals)}")
-    check(fn(_ptr(a), _ptr(a_vals), a.numel(), _ptr(b), _ptr(b_vals), b.numel(), _ptr(out), _ptr(out_vals),
-             ws, wsb, s), fn.__name__)
+    with torch.cuda.device(dev):
+        so = _stream_obj(stream, dev)
+        s = so.cuda_stream
+        ws, wsb = _ws("merge", tag, _payload_tag(a_vals), n, dev, so)
+        if a_vals is None:
+            fn = getattr(lib, f"bk_merge_{tag}")
+            check(fn(_ptr(a), a.numel(), _ptr(b), b.numel(), _ptr(out), ws, wsb, s), fn.__name__)
+            return out
+        fn = getattr(lib, f"bk_merge_by_key_{tag}_{_payload_tag(a_vals)}")
+        check(fn(_ptr(a), _ptr(a_vals), a.numel(), _ptr(b), _ptr(b_vals), b.numel(), _ptr(out), _ptr(out_vals),
+                 ws, wsb, s), fn.__name__)
     return out, out_vals
 
 
@@ -207,14 +222,16 @@ def stable_sort_by_key(keys: torch.Tensor, vals: torch.Tensor | None = None,
     n = keys.numel()
     if vals is not None and vals.numel() != n:
         raise ValueError("keys and vals must have the same length")
-    s = _stream_handle(stream, dev)
-    ws, wsb = _ws("sort_by_key", tag, _payload_tag(vals), n, dev, s)
-    if vals is None:
-        fn = getattr(lib, f"bk_sort_keys_{tag}")
-        check(fn(_ptr(keys), n, ws, wsb, s), fn.__name__)
-        return keys
-    fn = getattr(lib, f"bk_sort_by_key_{tag}_{_payload_tag(vals)}")
-    check(fn(_ptr(keys), _ptr(vals), n, ws, wsb, s), fn.__name__)
+    with torch.cuda.device(dev):
+        so = _stream_obj(stream, dev)
+        s = so.cuda_stream
+        ws, wsb = _ws("sort_by_key", tag, _payload_tag(vals), n, dev, so)
+        if vals is None:
+            fn = getattr(lib, f"bk_sort_keys_{tag}")
+            check(fn(_ptr(keys), n, ws, wsb, s), fn.__name__)
+            return keys
+        fn = getattr(lib, f"bk_sort_by_key_{tag}_{_payload_tag(vals)}")
+        check(fn(_ptr(keys), _ptr(vals), n, ws, wsb, s), fn.__name__)
     return keys, vals
 
 
@@ -239,10 +256,13 @@ def reduce_by_key(keys: torch.Tensor, vals: torch.Tensor, out_keys: torch.Tensor
         out_vals = torch.empty(max(n, 1), dtype=vals.dtype, device=dev)
     if num_out is None:
         num_out = torch.empty(1, dtype=torch.int64, device=dev)
-    s = _stream_handle(stream, dev)
-    ws, wsb = _ws("reduce_by_key", kt, vt, n, dev, s)
-    fn = getattr(lib, f"bk_reduce_by_key_{kt}_{vt}")
-    check(fn(_ptr(keys), _ptr(vals), n, _ptr(out_keys), _ptr(out_vals), _ptr(num_out), ws, wsb, s), fn.__name__)
+    with torch.cuda.device(dev):
+        so = _stream_obj(stream, dev)
+        s = so.cuda_stream
+        ws, wsb = _ws("reduce_by_key", kt, vt, n, dev, so)
+        fn = getattr(lib, f"bk_reduce_by_key_{kt}_{vt}")
+        check(fn(_ptr(keys), _ptr(vals), n, _ptr(out_keys), _ptr(out_vals), _ptr(num_out), ws, wsb, s),
+              fn.__name__)
     if not sync:
         return out_keys, out_vals, num_out
     c = int(num_out.item())

@@ -18,7 +18,7 @@ import torch
 
 from . import _lib
 from ._lib import check, lib
-from .algorithms import _require_cuda, _stream_handle, dtype_tag, workspaces
+from .algorithms import _require_cuda, _stream_obj, dtype_tag, workspaces
 
 BATCH_MAX = 256
 
@@ -74,7 +74,8 @@ def inclusive_scan_batch(xs, inits=None, outs=None, stream: torch.cuda.Stream | 
     outs = list(outs) if outs is not None else [torch.empty_like(x) for x in xs]
     if len(inits) != len(xs) or len(outs) != len(xs):
         raise ValueError("xs, inits and outs must have the same length")
-    s = _stream_handle(stream, dev)
+    so = _stream_obj(stream, dev)
+    s = so.cuda_stream
     item_t = scan_item_type(tag)
     fn = getattr(lib, f"bk_inclusive_scan_sum_{tag}_batch")
     for lo, hi in _chunks(len(xs)):
@@ -83,8 +84,9 @@ def inclusive_scan_batch(xs, inits=None, outs=None, stream: torch.cuda.Stream | 
             items[j].d_in, items[j].d_out, items[j].n, items[j].init = xs[k].data_ptr(), outs[k].data_ptr(), \
                 xs[k].numel(), inits[k]
         need = batch_workspace_bytes("inclusive_scan", tag, None, [xs[k].numel() for k in range(lo, hi)])
-        ws, wsb = workspaces.get(max(need, 256), dev, s)
-        check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
+        with torch.cuda.device(dev):
+            ws, wsb = workspaces.get(max(need, 256), dev, so)
+            check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
     return outs
 
 
@@ -109,7 +111,8 @@ def reduce_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | None =
             raise TypeError("one key dtype and one value dtype per batch")
         if k.numel() != v.numel():
             raise ValueError("keys and vals must have the same length")
-    s = _stream_handle(stream, dev)
+    so = _stream_obj(stream, dev)
+    s = so.cuda_stream
     item_t = rbk_item_type(kt, vt)
     fn = getattr(lib, f"bk_reduce_by_key_{kt}_{vt}_batch")
     if outs is not None:
@@ -134,8 +137,9 @@ def reduce_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | None =
             it.out_keys, it.out_vals = res[i][0].data_ptr(), res[i][1].data_ptr()
             it.d_num_out = cnt[i].data_ptr()
         need = batch_workspace_bytes("reduce_by_key", kt, vt, [keys_list[i].numel() for i in range(lo, hi)])
-        ws, wsb = workspaces.get(max(need, 256), dev, s)
-        check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
+        with torch.cuda.device(dev):
+            ws, wsb = workspaces.get(max(need, 256), dev, so)
+            check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
     if not sync:
         return [(ok, ov, cnt[i]) for i, (ok, ov) in enumerate(res)]
     cs = [int(c) for c in torch.cat([c.view(1) for c in cnt]).tolist()]
@@ -161,7 +165,8 @@ def stable_sort_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | N
             raise TypeError("one key dtype and one payload size per batch")
         if k.numel() != v.numel():
             raise ValueError("keys and vals must have the same length")
-    s = _stream_handle(stream, dev)
+    so = _stream_obj(stream, dev)
+    s = so.cuda_stream
     item_t = sort_item_type(kt, vt)
     fn = getattr(lib, f"bk_sort_by_key_{kt}_{vt}_batch")
     for lo, hi in _chunks(len(keys_list)):
@@ -170,6 +175,7 @@ def stable_sort_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | N
             items[j].keys, items[j].vals, items[j].n = keys_list[i].data_ptr(), vals_list[i].data_ptr(), \
                 keys_list[i].numel()
         need = batch_workspace_bytes("sort_by_key", kt, vt, [keys_list[i].numel() for i in range(lo, hi)])
-        ws, wsb = workspaces.get(max(need, 256), dev, s)
-        check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
+        with torch.cuda.device(dev):
+            ws, wsb = workspaces.get(max(need, 256), dev, so)
+            check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
     return keys_list, vals_list

@@ -13,6 +13,7 @@
 #include <limits>
 #include <type_traits>
 
+#include "bk_host_cache.hpp"
 #include "bulk_b200.h"
 
 namespace bk {
@@ -161,7 +162,6 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 
-// Record the first device-side error in the workspace header.
 // Asks L2 to fetch [p, p + bytes) from memory ahead of its use (nothing
 // reaches the SM).  The range is trimmed inward to 16-byte boundaries, so the
 // prefetch never leaves the caller's array.
@@ -176,6 +176,7 @@ __device__ __forceinline__ void prefetch_l2_range(const void *p, uint64_t bytes)
   }
 }
 
+// Record the first device-side error in the workspace header.
 __device__ __forceinline__ void record_error(WsHeader *h, int code, unsigned int tile) {
   if (atomicCAS(&h->status, 0, code) == 0) atomicExch(&h->err_tile, tile);
 }
@@ -355,6 +356,39 @@ inline int set_smem_attrs(Kern kern, size_t bytes) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
   return from_cuda(e);
+}
+
+// Runs setup(&value) once per device for the call site `Site` (a type unique
+// to the caller, such as a struct local to a function template), with that
+// device current, and caches the value only when setup returns BK_OK.
+// Kernel attributes and occupancy belong to a device, so the cache is keyed
+// by the current device, not by host thread.
+template <typename Site, typename T, typename F>
+inline int once_per_device(T *out, F &&setup) {
+  int dev = 0;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  return PerDevice<T, Site>::get(dev, out, setup, BK_ERR_UNSUPPORTED);
+}
+
+// One kernel's per-device launch facts.
+struct KernelSetup {
+  uint64_t resident_ctas;  // CTAs of it resident on the whole GPU at once
+};
+
+// Once per device for the call site `Site`: opts `kern` into `smem` bytes of
+// dynamic shared memory (and the largest carveout) and finds how many CTAs
+// of `threads` threads are resident on the GPU at once.
+template <typename Site, typename Kern>
+inline int kernel_setup(Kern kern, int threads, size_t smem, KernelSetup *out) {
+  return once_per_device<Site>(out, [&](KernelSetup *k) -> int {
+    DeviceInfo di;
+    int st = device_info(&di);
+    if (st != BK_OK) return st;
+    if ((st = set_smem_attrs(kern, smem)) != BK_OK) return st;
+    k->resident_ctas = resident_ctas(kern, threads, smem, di.sm_count);
+    return BK_OK;
+  });
 }
 
 }  // namespace host

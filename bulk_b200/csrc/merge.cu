@@ -101,14 +101,11 @@ int merge_launch(const K *a, const P *av, uint64_t na, const K *b, const P *bv, 
   st = host::launch_status();
   if (st != BK_OK) return st;
   constexpr size_t smem = merge_smem_bytes<K, P>();
-  static thread_local bool attr_set = false;
-  if (!attr_set) {
-    if ((st = host::set_smem_attrs(merge_kernel<K, P>, smem)) != BK_OK) return st;
-    attr_set = true;
-  }
-  static thread_local uint64_t ahead = 0;
-  if (ahead == 0) ahead = host::resident_ctas(merge_kernel<K, P>, kMergeThreads, smem, di.sm_count);
-  merge_kernel<K, P><<<(unsigned)tiles, kMergeThreads, smem, stream>>>(a, av, na, b, bv, nb, out, outv, parts, ahead);
+  struct Site {};
+  host::KernelSetup ks;
+  if ((st = host::kernel_setup<Site>(merge_kernel<K, P>, kMergeThreads, smem, &ks)) != BK_OK) return st;
+  merge_kernel<K, P><<<(unsigned)tiles, kMergeThreads, smem, stream>>>(a, av, na, b, bv, nb, out, outv, parts,
+                                                                       ks.resident_ctas);
   return host::launch_status();
 }
 

@@ -12,9 +12,11 @@
 // library holds it (1 MiB + 256 bytes) until the process exits.  Host code
 // cannot use the array's name as a device address (it names a host-side
 // shadow), so the device address is looked up with cudaGetSymbolAddress once
-// per device, with that device current, on the first call made on it.
-#include <mutex>
-
+// per device, with that device current, on the first call made on it (make
+// that first call before any stream capture).  Only a successful lookup is
+// kept: a failed one is tried again on the next call.  The kept address
+// belongs to the device's current context, so the entry point must not be
+// called on a device after cudaDeviceReset has destroyed that context.
 #include "bk_common.cuh"
 
 namespace {
@@ -26,29 +28,20 @@ constexpr size_t kNoAllocScratchBytes = 256 + (kNoAllocMaxN / 8192) * 8;
 
 static __device__ __align__(256) unsigned char g_noalloc_scan_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::once_flag g_once[kMaxDevices];
-void *g_scratch[kMaxDevices];
-int g_setup_status[kMaxDevices];
+struct NoAllocSite {};
 
 }  // namespace
 
 extern "C" int bk_inclusive_scan_sum_f32_noalloc(const float *d_in, uint64_t n, float init, float *d_out,
                                                  bk_stream_t stream) {
   if (n > kNoAllocMaxN) return BK_ERR_TOO_LARGE;
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return (int)e;
-  if (dev < 0 || dev >= kMaxDevices) return BK_ERR_UNSUPPORTED;
   // First call on this device (which is current): find the array's device address.
-  std::call_once(g_once[dev], [dev]() {
-    void *p = nullptr;
-    const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
-    g_scratch[dev] = p;
-    g_setup_status[dev] = (err == cudaSuccess) ? BK_OK : (int)err;
+  void *scratch = nullptr;
+  int st = bk::host::once_per_device<NoAllocSite>(&scratch, [](void **p) -> int {
+    return bk::host::from_cuda(cudaGetSymbolAddress(p, g_noalloc_scan_scratch));
   });
-  if (g_setup_status[dev] != BK_OK) return g_setup_status[dev];
-  void *scratch = g_scratch[dev];
+  if (st != BK_OK) return st;
+  cudaError_t e;
 
   const size_t need = bk_workspace_bytes(BK_ALGO_INCLUSIVE_SCAN, BK_DTYPE_F32, BK_DTYPE_NONE, n);
   if (need > kNoAllocScratchBytes) return BK_ERR_TOO_LARGE;

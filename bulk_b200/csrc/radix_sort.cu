@@ -412,18 +412,14 @@ int radix_sort_run(const Src &src, const RsLayout<K, P> &L, char *ws, cudaStream
   void *scan_ws = ws + L.scan_ws;
   auto *hdr = reinterpret_cast<WsHeader *>(ws);
   const auto *scan_hdr = reinterpret_cast<const WsHeader *>(scan_ws);
-  static thread_local bool attr_set = false;
-  static thread_local unsigned int up_ahead = 0, down_ahead = 0;
-  if (!attr_set) {
-    if ((st = host::set_smem_attrs(rs_downsweep_kernel<K, P, Src, kDownV, kDownTh>, rs_smem_bytes<K, P>())) != BK_OK)
-      return st;
-    host::DeviceInfo di;
-    if ((st = host::device_info(&di)) != BK_OK) return st;
-    up_ahead = (unsigned)host::resident_ctas(rs_upsweep_kernel<K, P, Src>, kRsThreads, 0, di.sm_count);
-    down_ahead = (unsigned)host::resident_ctas(rs_downsweep_kernel<K, P, Src, kDownV, kDownTh>, kDownTh,
-                                               rs_smem_bytes<K, P>(), di.sm_count);
-    attr_set = true;
-  }
+  struct UpSite {};
+  struct DownSite {};
+  host::KernelSetup up, down;
+  if ((st = host::kernel_setup<UpSite>(rs_upsweep_kernel<K, P, Src>, kRsThreads, 0, &up)) != BK_OK) return st;
+  if ((st = host::kernel_setup<DownSite>(rs_downsweep_kernel<K, P, Src, kDownV, kDownTh>, kDownTh,
+                                         rs_smem_bytes<K, P>(), &down)) != BK_OK)
+    return st;
+  const unsigned int up_ahead = (unsigned)up.resident_ctas, down_ahead = (unsigned)down.resident_ctas;
   // the scan's workspace must start zeroed, like any workspace
   if ((st = host::from_cuda(cudaMemsetAsync(scan_ws, 0, kHeaderBytes, stream))) != BK_OK) return st;
   for (int p = 0; p < rs_passes<K>(); ++p) {

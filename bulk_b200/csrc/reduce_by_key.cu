@@ -698,11 +698,9 @@ int rbk_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStrea
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
   const size_t smem = (size_t)kRbkBufs * C::BUF_BYTES;
-  static thread_local bool attr_set = false;
-  if (!attr_set) {
-    if ((st = host::set_smem_attrs(rbk_kernel<K, V, Src>, smem)) != BK_OK) return st;
-    attr_set = true;
-  }
+  struct Site {};
+  host::KernelSetup ks;
+  if ((st = host::kernel_setup<Site>(rbk_kernel<K, V, Src>, kRbkThreads, smem, &ks)) != BK_OK) return st;
   const unsigned grid = (unsigned)std::min<size_t>(tiles, std::min<size_t>((size_t)di.sm_count * 2, kRbkMaxGrid));
   V *ring = reinterpret_cast<V *>(reinterpret_cast<char *>(d_ws) + rbk_ring_offset<K, V>(tiles));
   rbk_kernel<K, V, Src><<<grid, kRbkThreads, smem, stream>>>(src, status, hdr, ring, limit, dbg.skip_publish_tile,

@@ -559,11 +559,9 @@ int scan_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStre
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
   const size_t smem = (size_t)kScanBufs * C::TILE_BYTES;
-  static thread_local bool attr_set = false;  // per host thread and kernel; cheap and idempotent
-  if (!attr_set) {
-    if ((st = host::set_smem_attrs(scan_kernel<T, Op, Src>, smem)) != BK_OK) return st;
-    attr_set = true;
-  }
+  struct Site {};
+  host::KernelSetup ks;
+  if ((st = host::kernel_setup<Site>(scan_kernel<T, Op, Src>, kScanThreads, smem, &ks)) != BK_OK) return st;
   const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * 2);
   scan_kernel<T, Op, Src><<<grid, kScanThreads, smem, stream>>>(src, status, hdr, limit, dbg.skip_publish_tile,
                                                                 (unsigned)tiles);

@@ -354,23 +354,21 @@ int sort_passes(uint64_t n) {
   return passes;
 }
 
-// Sets the kernels' shared-memory attributes once and returns (in *ahead)
+// Sets the kernels' shared-memory attributes once per device and returns (in *ahead)
 // how many merge-pass CTAs are resident at once.
 template <typename K, typename P, typename BsSrc, typename MpSrc>
 int sort_set_attrs(uint64_t *ahead) {
-  static thread_local bool attr_set = false;
-  static thread_local uint64_t mp_resident = 0;
-  if (!attr_set) {
+  struct Site {};
+  return host::once_per_device<Site>(ahead, [](uint64_t *mp_resident) -> int {
     int st;
     if ((st = set_smem(block_sort_kernel<K, P, BsSrc>, bs_smem_bytes<K, P>())) != BK_OK) return st;
     if ((st = set_smem(sort_merge_kernel<K, P, MpSrc>, mp_smem_bytes<K, P>())) != BK_OK) return st;
     host::DeviceInfo di;
     if ((st = host::device_info(&di)) != BK_OK) return st;
-    mp_resident = host::resident_ctas(sort_merge_kernel<K, P, MpSrc>, kMpThreads, mp_smem_bytes<K, P>(), di.sm_count);
-    attr_set = true;
-  }
-  *ahead = mp_resident;
-  return BK_OK;
+    *mp_resident =
+        host::resident_ctas(sort_merge_kernel<K, P, MpSrc>, kMpThreads, mp_smem_bytes<K, P>(), di.sm_count);
+    return BK_OK;
+  });
 }
 
 template <typename K, typename P>

@@ -7,7 +7,7 @@
 // group / agent, other args are passed by value; a stream policy launches
 // into that stream, a future policy into a new stream ordered after the
 // future, anything else into the legacy default stream.  The launch layer is
-// this library's own (SURVEY.md's rewrite of cuda_launcher / choose_sizes):
+// this library's own (in place of cuda_launcher / choose_sizes):
 //   parallel_group<agent<G>> of n agents   grid-stride loop, 256-thread CTAs,
 //                                          at most as many CTAs as are resident
 //                                          at once

@@ -2,7 +2,7 @@
 for the host (TEST INFRASTRUCTURE ONLY -- the checker and the timed CPU
 baseline; nothing in the product loads it).
 
-The recipe compiles the reference's headers where they lie (/root/reference,
+The recipe compiles the reference's headers where they lie (the reference checkout,
 read-only) after copying its bulk/ tree and decomposition.hpp into
 oracle/_ref/src (a build folder, kept out of git) and applying two patches to
 that copy:
@@ -31,7 +31,8 @@ ORACLE = HERE.parent
 OUT = ORACLE / "_ref"
 SRC = OUT / "src"
 LIB = OUT / "libbulkref.so"
-REFERENCE = Path(os.environ.get("BULK_REFERENCE", "/root/reference"))
+# the reference checkout: $BULK_REFERENCE, else the "reference" directory beside this repository
+REFERENCE = Path(os.environ.get("BULK_REFERENCE", str(ORACLE.parent.parent / "reference")))
 CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 
 PATCHES = [

@@ -4,9 +4,9 @@ It serves callers that cannot allocate device memory for a workspace (a
 plugin inside an application that owns all GPU memory, a latency-critical path
 that must not call cudaMalloc, an FFI caller without an allocator): its
 scratch is a fixed array inside the library.  This test calls it through the
-C-ABI twice in a row and checks each output against the regular workspace
-entry point (bk_inclusive_scan_sum_f32) within the float tolerance every scan
-test uses, 2*ceil(log2 n)*eps*sum|x|.  The file sorts last so that a run which
+C-ABI twice in a row and checks each output against the oracle's prefix sums
+and against the regular workspace entry point (bk_inclusive_scan_sum_f32),
+within the float tolerance every scan test uses, 2*ceil(log2 n)*eps*sum|x|.  The file sorts last so that a run which
 stops at the first failure has run every other test first; it also passes on
 its own in a fresh process.
 """
@@ -39,8 +39,9 @@ def test_noalloc_scan_matches_the_workspace_entry_point_twice(cuda, n):
         d = dev(x)
         got = host(_noalloc(d, 0.5))
         want = host(bulk_b200.inclusive_scan(d, np.float32(0.5)))
-        _, mag = oracle.inclusive_scan(x, np.float32(0.5))
-        assert_within_bound(got, want, mag, n, np.float32, f"noalloc call {call} n={n}")
+        ref, mag = oracle.inclusive_scan(x, np.float32(0.5))
+        assert_within_bound(got, ref, mag, n, np.float32, f"noalloc call {call} n={n} vs the oracle")
+        assert_within_bound(got, want, mag, n, np.float32, f"noalloc call {call} n={n} vs the workspace call")
 
 
 def test_noalloc_rejects_sizes_beyond_its_array():
