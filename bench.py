@@ -145,17 +145,28 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------
 def run_reference(args):
-    """CPU reference arm: the reference's reduce + scan structure on all host cores."""
+    """CPU reference arm: the reference's reduce + scan on all host cores,
+    over the full headline workload (N = 2^28 of each dtype)."""
     rank, world, _ = _env_rank()
     if rank != 0:
         return 0
-    line = cpu_reference_line(args.steps, args.warmup)
+    line = cpu_reference_line(args.steps, args.warmup, args.n)
     print(json.dumps(line), flush=True)
     return 0
 
 
+def cpu_model() -> str:
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_reference_time(n_sample: int, steps: int, warmup: int, threads: int):
-    """Seconds per sample-step of reduce + scan over n_sample elements of each
+    """Median seconds per step of reduce + scan over n_sample elements of each
     dtype, and which implementation ran ("reference": the reference's own
     algorithms compiled for the host, oracle/_ref; else "port": the oracle's
     threaded restatement)."""
@@ -192,34 +203,51 @@ def cpu_reference_time(n_sample: int, steps: int, warmup: int, threads: int):
 
     for _ in range(warmup):
         step()
-    if steps <= 0:  # size the sample to about 10 s of CPU work
+    times = []
+    for _ in range(max(1, steps)):
         t0 = time.perf_counter()
         step()
-        steps = int(min(50, max(1, 10.0 / max(time.perf_counter() - t0, 1e-3))))
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
-    return (time.perf_counter() - t0) / steps, kind, steps
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times), kind, len(times)
 
 
-def cpu_reference_line(steps, warmup):
-    """steps <= 0: as many sample steps as fill about 10 s."""
+def cpu_reference_line(steps, warmup, n=N_HEADLINE):
+    """The reference arm: every step is the whole headline workload (reduce +
+    inclusive_scan over n elements of each of f32 / f64 / i32) on all host
+    cores; value from the median step time."""
     threads = os.cpu_count() or 1
-    n_sample = 1 << 26
-    sec, kind, steps = cpu_reference_time(n_sample, steps, max(1, min(warmup, 3)), threads)
-    bytes_per = sum(3 * n_sample * s for _, s in DTYPES)
+    steps = max(1, min(steps, 10))
+    sec, kind, steps = cpu_reference_time(n, steps, max(1, min(warmup, 3)), threads)
+    bytes_per = sum(3 * n * s for _, s in DTYPES)
     gbs = bytes_per / sec / 1e9
     what = ("the reference's agent-level reduce / inclusive_scan compiled for the host, over the drivers' "
             "partitioning (reduce.cu, scan.cu)" if kind == "reference" else "the oracle's threaded restatement")
-    sample = (f"reduce+inclusive_scan over 2^26 elements of each of f32/f64/i32 (1/4 of the 2^28 workload), "
-              f"{threads} threads, {what}")
+    sample = (f"the full workload: reduce+inclusive_scan over {n} elements of each of f32/f64/i32, "
+              f"{threads} threads ({cpu_model()}), {what}; median of {steps} steps")
     return {"metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": 0, "steps": steps, "warmup": warmup,
-            "ms_per_step": sec * 1e3 * (N_HEADLINE / n_sample), "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64+i32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "n": N_HEADLINE, "l2": "inputs larger than L2"},
-            "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind,
-                             "sample": sample + f", {steps} timed sample steps"},
+            "config": {"workload": WORKLOAD, "n": n, "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind, "cpu_model": cpu_model(),
+                             "sample": sample},
             "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def cpu_baseline_object():
+    """The repo arm's cpu_baseline: the reference compiled for the host on all
+    host cores over a 2^26-element sample of each dtype (about 0.1-0.3 s per
+    step, median of 5), plus a 1-thread run over a 2^24-element sample."""
+    threads = os.cpu_count() or 1
+    n_all, n_one = 1 << 26, 1 << 24
+    sec, kind, steps = cpu_reference_time(n_all, 5, 1, threads)
+    sec1, _, steps1 = cpu_reference_time(n_one, 3, 1, 1)
+    per_elem = sum(3 * s for _, s in DTYPES)
+    gbs, gbs1 = per_elem * n_all / sec / 1e9, per_elem * n_one / sec1 / 1e9
+    return {"value": gbs, "unit": "GB/s", "cores": threads, "kind": kind, "cpu_model": cpu_model(),
+            "sample": (f"reduce+inclusive_scan over 2^26 elements of each of f32/f64/i32 (1/4 of the 2^28 "
+                       f"workload; GB/s is per byte, so it compares), {threads} threads, median of {steps} steps"),
+            "one_thread": {"value": gbs1, "unit": "GB/s", "cores": 1,
+                           "sample": f"the same over 2^24 elements of each dtype, 1 thread, median of {steps1} steps"}}
 
 
 # --------------------------------------------------------------------------
@@ -573,8 +601,7 @@ def main(argv=None):
         dist.destroy_process_group()
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
-            ref = cpu_reference_line(0, 1)
-            line["cpu_baseline"] = ref["cpu_baseline"]
+            line["cpu_baseline"] = cpu_baseline_object()
         print(json.dumps(line), flush=True)
     return 0
 

@@ -46,7 +46,8 @@ def _sources() -> list[Path]:
 
 
 def _deps() -> list[Path]:
-    return sorted(CSRC.glob("*.cuh")) + sorted((ROOT / "include").glob("*.h")) + [Path(__file__)]
+    return (sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + sorted(CSRC.glob("*.inc")) +
+            sorted((ROOT / "include").glob("*.h")) + [Path(__file__)])
 
 
 def _needs(target: Path, inputs: list[Path]) -> bool:

@@ -333,6 +333,13 @@ constexpr unsigned long long kDefaultSpinLimitNs = 2000000000ull;  // 2 s
 
 inline int from_cuda(cudaError_t e) { return e == cudaSuccess ? BK_OK : (int)e; }
 
+// Describes bytes [base, base + rows * 128) as a 2-D tensor of `rows` rows
+// of 128 bytes for tiled TMA loads of `box_rows` rows with the 128-byte
+// swizzle (`map` points at a 64-byte-aligned, 128-byte CUtensorMap).  base
+// must be 16-byte aligned and rows > 0.  The driver's encoder is looked up
+// once per process.
+int encode_rows_128b(void *map, const void *base, uint64_t rows, uint32_t box_rows);
+
 inline int check_ws(void *d_ws, size_t ws_bytes, size_t need) {
   if (need > 0 && d_ws == nullptr) return BK_ERR_INVALID_ARGUMENT;
   if (ws_bytes < need) return BK_ERR_WORKSPACE_TOO_SMALL;

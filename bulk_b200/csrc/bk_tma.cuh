@@ -1,12 +1,17 @@
 // bk_tma.cuh -- bulk (TMA) copies between global and shared memory, and the
 // mbarrier they complete on (sm_90+ PTX, used here for sm_100a).
 //
-// Only the untiled bulk forms are used: cp.async.bulk global->shared with an
-// mbarrier complete_tx, and cp.async.bulk shared->global with a bulk group.
-// No multicast form appears anywhere in this library.  Both addresses must be
-// 16-byte aligned and the size a multiple of 16 bytes; callers fetch ragged
-// edges with plain loads.
+// Two forms are used: the untiled cp.async.bulk (global->shared with an
+// mbarrier complete_tx, shared->global with a bulk group), whose addresses
+// must be 16-byte aligned and whose size is a multiple of 16 bytes (callers
+// fetch ragged edges with plain loads); and the tiled 2-D
+// cp.async.bulk.tensor load over a "row view" of a 1-D array (rows of 128
+// bytes, see host::encode_rows_128b) with the 128-byte swizzle, whose x
+// coordinate is always 0.  No multicast form appears anywhere in this
+// library.
 #pragma once
+
+#include <cuda.h>  // CUtensorMap (type only; the encoder comes from the driver at run time)
 
 #include "bk_common.cuh"
 
@@ -35,6 +40,14 @@ __device__ __forceinline__ void fence_proxy_async_global() {
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Adds `bytes` to the transaction count bar's current phase waits for,
+// without arriving (the arrival comes later, after any plain stores that the
+// waiting threads must also see).
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                : "memory");
 }
 
@@ -68,6 +81,26 @@ __device__ __forceinline__ void tma_load_1d_hint(void *smem_dst, const void *gme
       "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
       : "memory");
 }
+
+// Tiled 2-D copy global -> shared of the box at row `row` (x = 0) of the row
+// view `map` (a __grid_constant__ kernel parameter), with an L2 eviction
+// hint; completes the box's bytes on bar (rows past the view read as zero
+// and still count).  dst must be 1024-byte aligned for the 128-byte swizzle.
+__device__ __forceinline__ void tma_load_rows(void *smem_dst, const CUtensorMap *map, uint32_t row, uint64_t *bar,
+                                              uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_addr(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(smem_addr(bar)), "l"(policy)
+      : "memory");
+}
+
+// Byte offset at which a tensor copy with the 128-byte swizzle places byte
+// `o` of a 1024-byte-aligned box of 128-byte rows: the 16-byte chunk index
+// within each row is XORed with the row index mod 8, so eight lanes that
+// read the same chunk of eight consecutive rows hit eight distinct bank
+// groups.
+__host__ __device__ __forceinline__ uint32_t swz128(uint32_t o) { return o ^ (((o >> 7) & 7u) << 4); }
 
 // Bounded wait for phase `parity` of bar.  Returns false when the limit ran out.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned long long limit_ns) {

@@ -1,8 +1,11 @@
 // capi.cu -- library-wide C-ABI entry points: version, status strings,
-// workspace sizing / initialisation / status readback, device property cache
-// and the process-wide test hook.
+// workspace sizing / initialisation / status readback, device property cache,
+// the tensor-map encoder and the process-wide test hook.
 #include <atomic>
 #include <mutex>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "bk_common.cuh"
 
@@ -53,6 +56,35 @@ int device_info(DeviceInfo *out) {
 }
 
 DebugFault debug_fault() { return DebugFault{g_skip_tile.load(), g_spin_limit.load()}; }
+
+namespace {
+std::once_flag g_encode_once;
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+}  // namespace
+
+int encode_rows_128b(void *map, const void *base, uint64_t rows, uint32_t box_rows) {
+  std::call_once(g_encode_once, []() {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    else
+      (void)cudaGetLastError();
+  });
+  if (g_encode == nullptr) return BK_ERR_UNSUPPORTED;
+  if (rows == 0 || box_rows == 0 || box_rows > 256 || (reinterpret_cast<uintptr_t>(base) & 15) != 0)
+    return BK_ERR_INVALID_ARGUMENT;
+  const cuuint64_t dims[2] = {128, rows};
+  const cuuint64_t strides[1] = {128};
+  const cuuint32_t box[2] = {128, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = g_encode(reinterpret_cast<CUtensorMap *>(map), CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
+                              const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? BK_OK : BK_ERR_INVALID_ARGUMENT;
+}
 
 }  // namespace host
 }  // namespace bk

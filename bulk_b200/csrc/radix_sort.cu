@@ -30,6 +30,7 @@
 #include <type_traits>
 
 #include "bk_common.cuh"
+#include "bk_tune.hpp"
 #include "bk_merge.cuh"  // NoPayload, has_payload, payload_bytes
 #include "bulk_b200.h"
 
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_upsweep_kernel(const __grid_con
   __shared__ unsigned int s_wcnt[kRsWarps][kRsBins];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int shift = 8 * pass;
-  if (tid == 0) rs_prefetch_tile<K, P>(src, blockIdx.x + ahead, pass, false);
+  if (tid == 0 && ahead != 0) rs_prefetch_tile<K, P>(src, blockIdx.x + ahead, pass, false);
   const RsTile<K, P> tl = src.tile(blockIdx.x);
   const K *in_k = (pass & 1) ? tl.tk : tl.keys;
   const uint64_t tbase = (uint64_t)tl.local * kRsTile;
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downswe
     return;
   }
   const int shift = 8 * pass;
-  if (tid == 0) rs_prefetch_tile<K, P>(src, blockIdx.x + ahead, pass, true);
+  if (tid == 0 && ahead != 0) rs_prefetch_tile<K, P>(src, blockIdx.x + ahead, pass, true);
   const RsTile<K, P> tl = src.tile(blockIdx.x);
   const K *in_k = (pass & 1) ? tl.tk : tl.keys;
   const P *in_v = (pass & 1) ? tl.tv : tl.vals;
@@ -419,7 +420,10 @@ int radix_sort_run(const Src &src, const RsLayout<K, P> &L, char *ws, cudaStream
   if ((st = host::kernel_setup<DownSite>(rs_downsweep_kernel<K, P, Src, kDownV, kDownTh>, kDownTh,
                                          rs_smem_bytes<K, P>(), &down)) != BK_OK)
     return st;
-  const unsigned int up_ahead = (unsigned)up.resident_ctas, down_ahead = (unsigned)down.resident_ctas;
+  // L2 prefetch distance: the table's number of residencies ahead (0: none)
+  const tune::Knobs kn = tune::knobs_for(tune::kSort, (int)(sizeof(K) + payload_bytes<P>()), L.tiles * kRsTile);
+  const unsigned int up_ahead = (unsigned)up.resident_ctas * (unsigned)kn.prefetch;
+  const unsigned int down_ahead = (unsigned)down.resident_ctas * (unsigned)kn.prefetch;
   // the scan's workspace must start zeroed, like any workspace
   if ((st = host::from_cuda(cudaMemsetAsync(scan_ws, 0, kHeaderBytes, stream))) != BK_OK) return st;
   for (int p = 0; p < rs_passes<K>(); ++p) {

@@ -12,13 +12,16 @@
 // last CTA to finish (atomic counter) folds the partials in index order and
 // writes init (+) total to d_out.  The partition of the input depends only on
 // n and the SM count, so floating-point results repeat exactly run to run.
+#include <algorithm>
+
 #include "bk_common.cuh"
+#include "bk_tune.hpp"
 
 namespace bk {
 
 constexpr int kReduceThreads = 256;
 constexpr int kReduceUnroll = 8;
-constexpr int kReduceCtasPerSm = 4;
+constexpr int kReduceMaxCtasPerSm = 8;  // the largest grid the launch-shape table may pick
 
 template <typename T>
 struct ReduceLayout {
@@ -29,7 +32,7 @@ __host__ inline size_t reduce_partials_offset() { return kHeaderBytes; }
 
 template <typename T>
 size_t reduce_ws_bytes(int sm_count) {
-  return kHeaderBytes + align_up(sizeof(T) * (size_t)sm_count * kReduceCtasPerSm, 256);
+  return kHeaderBytes + align_up(sizeof(T) * (size_t)sm_count * kReduceMaxCtasPerSm, 256);
 }
 
 template <typename T, typename Op>
@@ -135,7 +138,8 @@ int reduce_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_
   const uint64_t tail = (n - head) - nvec * V;
   const uint64_t per_cta = (uint64_t)kReduceThreads * kReduceUnroll;
   uint64_t grid = (nvec + per_cta - 1) / per_cta;
-  const uint64_t max_grid = (uint64_t)di.sm_count * kReduceCtasPerSm;
+  const tune::Knobs kn = tune::knobs_for(tune::kReduce, (int)sizeof(T), n);
+  const uint64_t max_grid = (uint64_t)di.sm_count * (uint64_t)std::min(kn.ctas_per_sm, kReduceMaxCtasPerSm);
   if (grid > max_grid) grid = max_grid;
   if (grid < 1) grid = 1;
 

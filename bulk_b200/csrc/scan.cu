@@ -18,6 +18,7 @@
 // Semantics follow scan.cu:166-169 and bulk/algorithm/scan.hpp:455-486:
 // out[i] = init (+) in[0] (+) ... (+) in[i].
 #include "bk_common.cuh"
+#include "bk_tune.hpp"
 #include "bk_lookback.cuh"
 #include "bk_tma.cuh"
 
@@ -562,7 +563,9 @@ int scan_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStre
   struct Site {};
   host::KernelSetup ks;
   if ((st = host::kernel_setup<Site>(scan_kernel<T, Op, Src>, kScanThreads, smem, &ks)) != BK_OK) return st;
-  const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * 2);
+  const tune::Knobs kn = tune::knobs_for(tune::kScan, (int)sizeof(T), (uint64_t)tiles * C::TILE);
+  const unsigned grid =
+      (unsigned)std::min<size_t>(tiles, (size_t)di.sm_count * (size_t)std::min(std::max(kn.ctas_per_sm, 1), 2));
   scan_kernel<T, Op, Src><<<grid, kScanThreads, smem, stream>>>(src, status, hdr, limit, dbg.skip_publish_tile,
                                                                 (unsigned)tiles);
   return host::launch_status();

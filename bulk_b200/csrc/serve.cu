@@ -3,10 +3,16 @@
 //
 // No counterpart in the reference, whose drivers run one array at a time.
 // The loop is host code over the C-ABI: admission against an HBM budget, a
-// pooled allocator over one caller-owned device buffer, issue on one stream,
-// completion by event polling, and per-request start / done times on the
-// host's steady clock.  Its one kernel gathers the sort requests' input
-// windows into their own buffers for a whole batch in a single launch.
+// pooled allocator over one caller-owned device buffer, completion by event
+// polling, and per-request start / done times on the host's steady clock.
+// Plain mode issues everything on the caller's stream.  Batched mode issues
+// each admission round as one batch per request kind, the kinds on three
+// streams of their own (forked from the caller's stream and joined back to
+// it, each with its own slice of the workspace) so that a round's sorts,
+// reduce_by_keys and scans run side by side on the device; a kind with a
+// single request in the round is issued as a plain single-array call.  Its
+// one kernel gathers the sort requests' input windows into their own
+// buffers for a whole batch in a single launch.
 #include <algorithm>
 #include <chrono>
 #include <deque>
@@ -126,15 +132,38 @@ uint64_t request_bytes(uint32_t kind, uint64_t n) {
   return (kind == BK_SERVE_SCAN ? 4 : 8) * n + 512;
 }
 
+// Batched mode: the workspace holds one slice per request kind (the kinds'
+// batches run on separate streams at once), each a multiple of 256 bytes.
+struct WsSlices {
+  size_t off[3];
+  size_t bytes[3];
+  size_t total;
+};
+WsSlices batched_slices(const bk_serve_request *reqs, uint32_t count);
+
 class Loop {
  public:
   Loop(const bk_serve_config &c, uint64_t count) : c_(c), pool_(c.pool_bytes) {
     (void)count;
     st_ = reinterpret_cast<cudaStream_t>(c.stream);
     base_ = reinterpret_cast<char *>(c.pool);
+    for (int k = 0; k < 3; ++k) ks_[k] = nullptr;
   }
   ~Loop() {
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
+    for (int k = 0; k < 3; ++k)
+      if (ks_[k]) cudaStreamDestroy(ks_[k]);
+  }
+
+  // Batched mode: the kinds' streams and workspace slices.
+  int setup_batched(const WsSlices &sl) {
+    for (int k = 0; k < 3; ++k) {
+      const cudaError_t e = cudaStreamCreateWithFlags(&ks_[k], cudaStreamNonBlocking);
+      if (e != cudaSuccess) return host::from_cuda(e);
+      ws_[k] = static_cast<char *>(c_.ws) + sl.off[k];
+      ws_bytes_[k] = sl.bytes[k];
+    }
+    return BK_OK;
   }
 
   int run(const bk_serve_request *reqs, uint32_t count, bk_serve_record *recs, bk_serve_stats *stats) {
@@ -168,17 +197,12 @@ class Loop {
       }
       // arrivals and admission, in arrival order
       const double ta = now();
-      bool blocked = false;
       while (next < count && all[next].r->arrival_s <= ta) {
         const int a = admit(&all[next]);
-        if (a == 0) {
-          blocked = true;
-          break;
-        }
+        if (a == 0) break;  // over budget: wait for completions
         if (a < 0) {
           // cannot fit even with nothing else admitted
           if (admitted_ == 0 && inflight.empty() && waiting.empty()) return finish(BK_ERR_TOO_LARGE, stats, t0);
-          blocked = true;
           break;
         }
         Req *r = &all[next++];
@@ -192,7 +216,6 @@ class Loop {
           waiting.push_back(r);
         }
       }
-      (void)blocked;
       if (c_.mode == BK_SERVE_BATCHED && !waiting.empty() && (int)inflight.size() < c_.max_inflight) {
         const double ti = now();
         for (Req *r : waiting) r->rec->start_s = ti;
@@ -208,6 +231,13 @@ class Loop {
 
  private:
   int finish(int st, bk_serve_stats *stats, std::chrono::steady_clock::time_point t0) {
+    // the kinds' streams first: after a failure mid-round they may hold work
+    // that was never joined to the caller's stream
+    for (int k = 0; k < 3; ++k) {
+      if (ks_[k] == nullptr) continue;
+      const cudaError_t ek = cudaStreamSynchronize(ks_[k]);
+      if (st == BK_OK) st = host::from_cuda(ek);
+    }
     const cudaError_t e = cudaStreamSynchronize(st_);
     if (st == BK_OK) st = host::from_cuda(e);
     if (stats) {
@@ -219,7 +249,9 @@ class Loop {
     return st;
   }
 
-  int record(cudaEvent_t *ev) {
+  int record(cudaEvent_t *ev) { return record_on(ev, st_); }
+
+  int record_on(cudaEvent_t *ev, cudaStream_t s) {
     if (free_events_.empty()) {
       cudaEvent_t e;
       const cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
@@ -229,7 +261,15 @@ class Loop {
     }
     *ev = free_events_.back();
     free_events_.pop_back();
-    return host::from_cuda(cudaEventRecord(*ev, st_));
+    return host::from_cuda(cudaEventRecord(*ev, s));
+  }
+
+  // Fork/join helper events are reusable once the stream that waits on them
+  // has been told to: a later record only affects later waits.
+  int helper_event(cudaEvent_t *ev, cudaStream_t s) {
+    const int st = record_on(ev, s);
+    free_events_.push_back(*ev);
+    return st;
   }
 
   // 1 admitted, 0 over budget (wait), -1 the pool has no room (wait, or fail
@@ -268,38 +308,73 @@ class Loop {
     return reinterpret_cast<T *>(base_ + q->off[i]);
   }
 
-  int issue_one(Req *q) {
+  // One request as its own single-array call on stream s with workspace ws.
+  int issue_one(Req *q) { return issue_one_on(q, st_, c_.ws, c_.ws_bytes); }
+
+  int issue_one_on(Req *q, cudaStream_t s, void *ws, size_t ws_bytes) {
     const uint64_t n = q->r->n, o = q->r->src_offset;
     ++calls_;
     switch (q->r->kind) {
       case BK_SERVE_SORT: {
         uint32_t *k = buf<uint32_t>(q, 0), *v = buf<uint32_t>(q, 1);
-        cudaError_t e = cudaMemcpyAsync(k, c_.sort_keys + o, 4 * n, cudaMemcpyDeviceToDevice, st_);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(v, c_.sort_vals + o, 4 * n, cudaMemcpyDeviceToDevice, st_);
+        cudaError_t e = cudaMemcpyAsync(k, c_.sort_keys + o, 4 * n, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(v, c_.sort_vals + o, 4 * n, cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return host::from_cuda(e);
-        return bk_sort_by_key_u32_u32(k, v, n, c_.ws, c_.ws_bytes, c_.stream);
+        return bk_sort_by_key_u32_u32(k, v, n, ws, ws_bytes, (bk_stream_t)s);
       }
       case BK_SERVE_RBK:
         return bk_reduce_by_key_i32_f32(c_.rbk_keys + o, c_.rbk_vals + o, n, buf<int32_t>(q, 0), buf<float>(q, 1),
-                                        buf<uint64_t>(q, 2), c_.ws, c_.ws_bytes, c_.stream);
+                                        buf<uint64_t>(q, 2), ws, ws_bytes, (bk_stream_t)s);
       default:
-        return bk_inclusive_scan_sum_f32(c_.scan_vals + o, n, 0.0f, buf<float>(q, 0), c_.ws, c_.ws_bytes, c_.stream);
+        return bk_inclusive_scan_sum_f32(c_.scan_vals + o, n, 0.0f, buf<float>(q, 0), ws, ws_bytes, (bk_stream_t)s);
     }
   }
 
-  // One batched call per kind (at most BK_BATCH_MAX arrays each); the sort
-  // inputs are gathered first, 128 requests (256 copies) per launch.
+  // One admission round: per kind, one batched call (at most BK_BATCH_MAX
+  // arrays each; the sort inputs gathered first, 128 requests per gather
+  // launch), or a plain call for a kind with one request.  With more than
+  // one kind present, each kind runs on its own stream, forked from the
+  // caller's stream and joined back to it; otherwise the kind runs on the
+  // caller's stream (its slice is free there: the caller's stream has
+  // joined every earlier use of it).
   int issue_batches(const std::vector<Req *> &reqs) {
     std::vector<Req *> by[3];
     for (Req *r : reqs) by[r->r->kind].push_back(r);
+    const int kinds = (by[0].empty() ? 0 : 1) + (by[1].empty() ? 0 : 1) + (by[2].empty() ? 0 : 1);
     int st;
-    for (size_t lo = 0; lo < by[BK_SERVE_SORT].size(); lo += kGatherMax / 2) {
-      const size_t hi = std::min(by[BK_SERVE_SORT].size(), lo + kGatherMax / 2);
+    cudaEvent_t fork = nullptr;
+    if (kinds > 1 && (st = helper_event(&fork, st_)) != BK_OK) return st;
+    for (int kind = 0; kind < 3; ++kind) {
+      if (by[kind].empty()) continue;
+      cudaStream_t s = st_;
+      if (kinds > 1) {
+        s = ks_[kind];
+        if ((st = host::from_cuda(cudaStreamWaitEvent(s, fork, 0))) != BK_OK) return st;
+      }
+      if (by[kind].size() == 1) st = issue_one_on(by[kind][0], s, ws_[kind], ws_bytes_[kind]);
+      else st = issue_kind(kind, by[kind], s);
+      if (st != BK_OK) return st;
+      if (kinds > 1) {
+        cudaEvent_t join;
+        if ((st = helper_event(&join, s)) != BK_OK) return st;
+        if ((st = host::from_cuda(cudaStreamWaitEvent(st_, join, 0))) != BK_OK) return st;
+      }
+    }
+    return BK_OK;
+  }
+
+  // One kind's batched calls on stream s with the kind's workspace slice.
+  int issue_kind(int kind, const std::vector<Req *> &v, cudaStream_t s) {
+    int st;
+    void *ws = ws_[kind];
+    const size_t wsb = ws_bytes_[kind];
+    for (size_t lo = 0; kind == BK_SERVE_SORT && lo < v.size(); lo += kGatherMax / 2) {
+      const size_t hi = std::min(v.size(), lo + kGatherMax / 2);
       GatherBatch g;
       g.count = 0;
       g.units[0] = 0;
       for (size_t i = lo; i < hi; ++i) {
-        const Req *q = by[BK_SERVE_SORT][i];
+        const Req *q = v[i];
         const uint64_t n = q->r->n, o = q->r->src_offset;
         const uint32_t *srcs[2] = {c_.sort_keys + o, c_.sort_vals + o};
         for (int b = 0; b < 2; ++b) {
@@ -313,36 +388,33 @@ class Loop {
       const uint64_t units = g.units[g.count];
       if (units == 0) continue;
       const unsigned grid = (unsigned)std::min<uint64_t>((units + 255) / 256, 148ull * 8);
-      gather_kernel<<<grid, 256, 0, st_>>>(g);
+      gather_kernel<<<grid, 256, 0, s>>>(g);
       if ((st = host::launch_status()) != BK_OK) return st;
     }
-    for (int kind = 0; kind < 3; ++kind) {
-      const std::vector<Req *> &v = by[kind];
-      for (size_t lo = 0; lo < v.size(); lo += BK_BATCH_MAX) {
-        const size_t hi = std::min(v.size(), lo + (size_t)BK_BATCH_MAX);
-        ++calls_;
-        ++batches_;
-        if (kind == BK_SERVE_SORT) {
-          bk_sort_item_u32_u32 it[BK_BATCH_MAX];
-          for (size_t i = lo; i < hi; ++i)
-            it[i - lo] = bk_sort_item_u32_u32{buf<uint32_t>(v[i], 0), buf<uint32_t>(v[i], 1), v[i]->r->n};
-          st = bk_sort_by_key_u32_u32_batch(it, (uint32_t)(hi - lo), c_.ws, c_.ws_bytes, c_.stream);
-        } else if (kind == BK_SERVE_RBK) {
-          bk_rbk_item_i32_f32 it[BK_BATCH_MAX];
-          for (size_t i = lo; i < hi; ++i) {
-            const uint64_t o = v[i]->r->src_offset;
-            it[i - lo] = bk_rbk_item_i32_f32{c_.rbk_keys + o, c_.rbk_vals + o, v[i]->r->n, buf<int32_t>(v[i], 0),
-                                            buf<float>(v[i], 1), buf<uint64_t>(v[i], 2)};
-          }
-          st = bk_reduce_by_key_i32_f32_batch(it, (uint32_t)(hi - lo), c_.ws, c_.ws_bytes, c_.stream);
-        } else {
-          bk_scan_item_f32 it[BK_BATCH_MAX];
-          for (size_t i = lo; i < hi; ++i)
-            it[i - lo] = bk_scan_item_f32{c_.scan_vals + v[i]->r->src_offset, buf<float>(v[i], 0), v[i]->r->n, 0.0f};
-          st = bk_inclusive_scan_sum_f32_batch(it, (uint32_t)(hi - lo), c_.ws, c_.ws_bytes, c_.stream);
+    for (size_t lo = 0; lo < v.size(); lo += BK_BATCH_MAX) {
+      const size_t hi = std::min(v.size(), lo + (size_t)BK_BATCH_MAX);
+      ++calls_;
+      ++batches_;
+      if (kind == BK_SERVE_SORT) {
+        bk_sort_item_u32_u32 it[BK_BATCH_MAX];
+        for (size_t i = lo; i < hi; ++i)
+          it[i - lo] = bk_sort_item_u32_u32{buf<uint32_t>(v[i], 0), buf<uint32_t>(v[i], 1), v[i]->r->n};
+        st = bk_sort_by_key_u32_u32_batch(it, (uint32_t)(hi - lo), ws, wsb, (bk_stream_t)s);
+      } else if (kind == BK_SERVE_RBK) {
+        bk_rbk_item_i32_f32 it[BK_BATCH_MAX];
+        for (size_t i = lo; i < hi; ++i) {
+          const uint64_t o = v[i]->r->src_offset;
+          it[i - lo] = bk_rbk_item_i32_f32{c_.rbk_keys + o, c_.rbk_vals + o, v[i]->r->n, buf<int32_t>(v[i], 0),
+                                          buf<float>(v[i], 1), buf<uint64_t>(v[i], 2)};
         }
-        if (st != BK_OK) return st;
+        st = bk_reduce_by_key_i32_f32_batch(it, (uint32_t)(hi - lo), ws, wsb, (bk_stream_t)s);
+      } else {
+        bk_scan_item_f32 it[BK_BATCH_MAX];
+        for (size_t i = lo; i < hi; ++i)
+          it[i - lo] = bk_scan_item_f32{c_.scan_vals + v[i]->r->src_offset, buf<float>(v[i], 0), v[i]->r->n, 0.0f};
+        st = bk_inclusive_scan_sum_f32_batch(it, (uint32_t)(hi - lo), ws, wsb, (bk_stream_t)s);
       }
+      if (st != BK_OK) return st;
     }
     return BK_OK;
   }
@@ -350,6 +422,9 @@ class Loop {
   const bk_serve_config c_;
   Pool pool_;
   cudaStream_t st_;
+  cudaStream_t ks_[3];   // batched mode: one stream per request kind
+  void *ws_[3] = {nullptr, nullptr, nullptr};
+  size_t ws_bytes_[3] = {0, 0, 0};
   char *base_;
   uint64_t admitted_ = 0;
   uint64_t calls_ = 0, batches_ = 0;
@@ -389,8 +464,23 @@ extern "C" size_t bk_serve_workspace_bytes(const bk_serve_request *reqs, uint32_
     }
     return need;
   }
-  // batched: a batch's workspace grows with its arrays, so the largest
-  // BK_BATCH_MAX requests of a kind bound every batch of that kind
+  for (uint32_t i = 0; i < count; ++i)
+    if (reqs[i].kind > BK_SERVE_SCAN) return 0;
+  return std::max(need, bk::serve::batched_slices(reqs, count).total);
+}
+
+namespace bk {
+namespace serve {
+// Batched mode: one workspace slice per kind (the kinds run at once on their
+// own streams).  A batch's workspace grows with its arrays, so the largest
+// BK_BATCH_MAX requests of a kind bound every batch of that kind; a slice
+// also covers the kind's largest request run alone.
+WsSlices batched_slices(const bk_serve_request *reqs, uint32_t count) {
+  static const int algo[3] = {BK_ALGO_SORT_BY_KEY, BK_ALGO_REDUCE_BY_KEY, BK_ALGO_INCLUSIVE_SCAN};
+  static const int key[3] = {BK_DTYPE_U32, BK_DTYPE_I32, BK_DTYPE_F32};
+  static const int val[3] = {BK_DTYPE_U32, BK_DTYPE_F32, BK_DTYPE_NONE};
+  WsSlices sl{};
+  size_t off = 0;
   for (uint32_t k = 0; k < 3; ++k) {
     std::vector<uint64_t> sizes;
     for (uint32_t i = 0; i < count; ++i)
@@ -399,10 +489,19 @@ extern "C" size_t bk_serve_workspace_bytes(const bk_serve_request *reqs, uint32_
       std::nth_element(sizes.begin(), sizes.begin() + BK_BATCH_MAX, sizes.end(), std::greater<uint64_t>());
       sizes.resize(BK_BATCH_MAX);
     }
-    need = std::max(need, bk_batch_workspace_bytes(algo[k], key[k], val[k], sizes.data(), (uint32_t)sizes.size()));
+    size_t need = std::max<size_t>(
+        bk::kHeaderBytes, bk_batch_workspace_bytes(algo[k], key[k], val[k], sizes.data(), (uint32_t)sizes.size()));
+    for (uint64_t n : sizes) need = std::max(need, bk_workspace_bytes(algo[k], key[k], val[k], n));
+    need = bk::align_up(need, 256);
+    sl.off[k] = off;
+    sl.bytes[k] = need;
+    off += need;
   }
-  return need;
+  sl.total = off;
+  return sl;
 }
+}  // namespace serve
+}  // namespace bk
 
 extern "C" int bk_serve_run(const bk_serve_config *cfg, const bk_serve_request *reqs, uint32_t count,
                             bk_serve_record *records, bk_serve_stats *stats) {
@@ -419,6 +518,16 @@ extern "C" int bk_serve_run(const bk_serve_config *cfg, const bk_serve_request *
   if (c.ws_bytes < bk_serve_workspace_bytes(reqs, count, c.mode)) return BK_ERR_WORKSPACE_TOO_SMALL;
   for (uint32_t i = 0; i < count; ++i) records[i] = bk_serve_record{-1.0, -1.0, {0, 0, 0}};
   bk::serve::Loop loop(c, count);
+  if (c.mode == BK_SERVE_BATCHED) {
+    // each slice is a workspace of its own: its header (the counters every
+    // call leaves at zero) must start zeroed
+    const bk::serve::WsSlices sl = bk::serve::batched_slices(reqs, count);
+    for (int k = 0; k < 3; ++k)
+      if ((st = bk::host::from_cuda(cudaMemsetAsync(static_cast<char *>(c.ws) + sl.off[k], 0, bk::kHeaderBytes,
+                                                    (cudaStream_t)c.stream))) != BK_OK)
+        return st;
+    if ((st = loop.setup_batched(sl)) != BK_OK) return st;
+  }
   return loop.run(reqs, count, records, stats);
 }
 

@@ -23,6 +23,7 @@
 
 #include <cuda/std/tuple>
 #include <cuda/std/utility>
+#include <thrust/tuple.h>
 
 #include "execution_policy.hpp"
 #include "malloc.hpp"
@@ -254,6 +255,47 @@ __device__ T reduce(concurrent_group<A, S> &g, It first, It last, T init, Op op)
 
 template <typename A, std::size_t S, typename It, typename T, typename Op>
 __device__ T accumulate(concurrent_group<A, S> &g, It first, It last, T init, Op op) {
+  return reduce(g, first, last, init, op);
+}
+
+// A cluster group (a concurrent group of C CTAs) reduces in order: CTA r
+// folds its contiguous share of the range with the CTA-wide ordered scan and
+// leaves the result in its shared memory; after a cluster barrier every
+// agent folds the C results in rank order, reading the other CTAs' shared
+// memory through the cluster window.  Every agent receives the result.
+template <typename A, std::size_t S, std::size_t C, typename It, typename T, typename Op>
+__device__ T reduce(concurrent_group<concurrent_group<A, S>, C> &g, It first, It last, T init, Op op) {
+  __shared__ __align__(16) unsigned char s_part[sizeof(T)];
+  __shared__ int s_part_has;
+  const long long n = last - first;
+  const int r = g.this_exec.index(), size = g.this_exec.size(), t = g.this_exec.this_exec.index();
+  const long long share = (n + (long long)C - 1) / (long long)C;
+  const long long lo = detail::min_((long long)r * share, n), hi = detail::min_(lo + share, n);
+  const long long chunk = (hi - lo + size - 1) / size;
+  const long long a0 = detail::min_(lo + (long long)t * chunk, hi), a1 = detail::min_(a0 + chunk, hi);
+  detail::opt<T> local{T(), false};
+  for (long long i = a0; i < a1; ++i) local = detail::opt<T>{local.has ? op(local.v, first[i]) : T(first[i]), true};
+  detail::opt<T> total;
+  (void)detail::cta_exclusive_scan(local, op, &total);
+  if (t == 0) {
+    memcpy(s_part, &total.v, sizeof(T));
+    s_part_has = total.has ? 1 : 0;
+  }
+  g.wait();  // every CTA's result is in place
+  T acc = init;
+  for (int q = 0; q < (int)C; ++q) {
+    if (*detail::cluster_map(&s_part_has, (unsigned)q)) {
+      T v;
+      memcpy(&v, detail::cluster_map(&s_part[0], (unsigned)q), sizeof(T));
+      acc = op(acc, v);
+    }
+  }
+  g.wait();  // every agent has read them before any CTA reuses its slot
+  return acc;
+}
+
+template <typename A, std::size_t S, std::size_t C, typename It, typename T, typename Op>
+__device__ T accumulate(concurrent_group<concurrent_group<A, S>, C> &g, It first, It last, T init, Op op) {
   return reduce(g, first, last, init, op);
 }
 
@@ -562,7 +604,7 @@ __device__ void stable_sort(bounded<bound, concurrent_group<A, S>> &g, It first,
 // the new carry: (keys_result end, values_result end, carry key, carry value).
 template <typename A, std::size_t S, typename KIt, typename VIt, typename KOut, typename VOut, typename T1,
           typename T2, typename Pred, typename Op>
-__device__ cuda::std::tuple<KOut, VOut, detail::value_t<KIt>, detail::value_t<VOut>> reduce_by_key(
+__device__ thrust::tuple<KOut, VOut, detail::value_t<KIt>, detail::value_t<VOut>> reduce_by_key(
     concurrent_group<A, S> &g, KIt keys_first, KIt keys_last, VIt values_first, KOut keys_result, VOut values_result,
     T1 init_key, T2 init_value, Pred pred, Op op) {
   typedef detail::value_t<KIt> K;
@@ -622,7 +664,7 @@ __device__ cuda::std::tuple<KOut, VOut, detail::value_t<KIt>, detail::value_t<VO
     carry.c = 0;
   }
   g.wait();
-  return cuda::std::make_tuple(keys_result + emitted, values_result + emitted, carry_key, carry.v);
+  return thrust::make_tuple(keys_result + emitted, values_result + emitted, carry_key, carry.v);
 }
 
 }  // namespace bulk

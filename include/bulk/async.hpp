@@ -55,7 +55,7 @@ inline device_props device_properties() {
   static device_props props[64];
   int dev = 0;
   throw_on_error(cudaGetDevice(&dev), "bulk: cudaGetDevice");
-  if (dev < 0 || dev >= 64) throw std::runtime_error("bulk: device index out of range");
+  if (dev < 0 || dev >= 64) throw_on_error(cudaErrorInvalidDevice, "bulk: device index out of range");
   std::call_once(once[dev], [dev]() {
     device_props p{};
     cudaDeviceGetAttribute(&p.sm_count, cudaDevAttrMultiProcessorCount, dev);
@@ -133,6 +133,38 @@ __global__ void async_grid_of_groups(int num_groups, Group proto, unsigned int h
   invoke(root, f, a, std::index_sequence_for<Args...>());
 }
 
+template <typename T>
+struct is_cluster_group : std::false_type {};
+template <typename A, std::size_t S, std::size_t C>
+struct is_cluster_group<concurrent_group<concurrent_group<A, S>, C>> : std::true_type {};
+
+// A grid of clusters (AS_GRID: the root is parallel_group<Cluster> of
+// num_clusters clusters) or one cluster (the cluster group is the root).
+// Every CTA initialises its heap and the cluster meets once before the
+// functor runs (a peer may allocate from this CTA's heap) and once after it
+// (no CTA leaves while a peer may still use its shared memory).
+template <bool AS_GRID, typename Cluster, typename F, typename... Args>
+__global__ void async_cluster_groups(int num_clusters, Cluster proto, unsigned int heap_bytes, F f, Args... args) {
+  if (threadIdx.x == 0) heap_init(heap_bytes);
+  cluster_barrier();
+  {
+    cuda::std::tuple<Args...> a(args...);
+    typedef typename Cluster::agent_type cta_type;
+    typedef typename cta_type::agent_type agent_type;
+    const int rank = (int)cluster_ctarank();
+    const int cluster_index = (int)(blockIdx.x / cluster_nctarank());
+    cta_type cta = make_group(proto.this_exec, agent_type(threadIdx.x), rank);
+    Cluster cl(cta, cluster_index);
+    if constexpr (AS_GRID) {
+      parallel_group<Cluster> root(num_clusters, cl, 0);
+      invoke(root, f, a, std::index_sequence_for<Args...>());
+    } else {
+      invoke(cl, f, a, std::index_sequence_for<Args...>());
+    }
+  }
+  cluster_barrier();
+}
+
 // Default heap: the share of an SM's shared memory that keeps every group
 // that fits by thread count resident.
 inline unsigned int choose_heap(int group_size, int requested) {
@@ -165,10 +197,54 @@ inline int resident_per_sm(Kernel k, int threads, size_t smem) {
   return per_sm;
 }
 
+// Launches `num_clusters` clusters of C CTAs (grid = num_clusters * C) with
+// cudaLaunchKernelEx and a cluster dimension; above 8 CTAs per cluster the
+// kernel is opted into non-portable cluster sizes.  num_clusters == 0 asks
+// for the number of clusters resident at once (occupancy of this kernel).
+template <bool AS_GRID, typename Cluster, typename F, typename... Args>
+void launch_clusters(int num_clusters, const Cluster &g_in, cudaStream_t s, F f, Args... args) {
+  constexpr int C = (int)Cluster::static_size;
+  typedef typename Cluster::agent_type cta_type;
+  const cta_type &inner = g_in.this_exec;
+  const int size = default_group_size(inner.size());
+  const unsigned int heap = choose_heap(size, inner.heap_size());
+  Cluster proto(make_group_size(inner, size, (int)heap), 0);
+  auto k = async_cluster_groups<AS_GRID, Cluster, F, Args...>;
+  opt_in_smem(k, heap);
+  if (C > 8)
+    throw_on_error(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+                   "bulk::async: non-portable cluster size");
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(size);
+  cfg.dynamicSmemBytes = heap;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (num_clusters == use_default) {
+    cfg.gridDim = dim3(C);
+    int resident = 0;
+    throw_on_error(cudaOccupancyMaxActiveClusters(&resident, k, &cfg), "bulk::async: cluster occupancy");
+    num_clusters = resident > 0 ? resident : 1;
+  }
+  if (num_clusters <= 0) return;
+  cfg.gridDim = dim3((unsigned)num_clusters * C);
+  throw_on_error(cudaLaunchKernelEx(&cfg, k, num_clusters, proto, heap, f, args...),
+                 "bulk::async: cluster launch");
+}
+
 // ---- launch into a stream ----------------------------------------------------
 template <typename Agent, std::size_t N, typename F, typename... Args>
 void launch(const parallel_group<Agent, N> &g, cudaStream_t s, F f, Args... args) {
-  if constexpr (is_concurrent_group<Agent>::value) {
+  if constexpr (is_cluster_group<Agent>::value) {
+    // a grid of clusters
+    launch_clusters<true>(g.size(), g.this_exec, s, f, args...);
+    return;
+  } else if constexpr (is_concurrent_group<Agent>::value) {
     // a grid of concurrent groups (one CTA each)
     const Agent &proto_in = g.this_exec;
     const int size = default_group_size(proto_in.size());
@@ -188,6 +264,12 @@ void launch(const parallel_group<Agent, N> &g, cudaStream_t s, F f, Args... args
     if (n > 0) k<<<blocks, threads, 0, s>>>(n, f, args...);
   }
   throw_on_error(cudaGetLastError(), "bulk::async: launch");
+}
+
+// one cluster of C CTAs
+template <typename A, std::size_t S, std::size_t C, typename F, typename... Args>
+void launch(const concurrent_group<concurrent_group<A, S>, C> &g, cudaStream_t s, F f, Args... args) {
+  launch_clusters<false>(1, g, s, f, args...);
 }
 
 template <typename A, std::size_t S, typename F, typename... Args>

@@ -10,8 +10,13 @@
 //   agent                       one CUDA thread (grainsize is a hint)
 //   concurrent_group<A, S>      one CTA of S threads; wait() is a CTA barrier;
 //                               the heap is the CTA's dynamic shared memory
+//   concurrent_group<concurrent_group<A, S>, C>
+//                               a thread-block cluster of C CTAs (C <= 16);
+//                               wait() is a cluster barrier; each CTA's heap
+//                               falls back to its peers' shared memory
+//                               (distributed shared memory)
 //   parallel_group<A>           independent agents: a grid-stride launch
-//   parallel_group<concurrent_group<...>>  a grid of CTAs
+//   parallel_group<concurrent_group<...>>  a grid of CTAs (or of clusters)
 #pragma once
 
 #include <climits>
@@ -199,6 +204,55 @@ class concurrent_group<ExecutionAgent, dynamic_group_size>
   size_type m_heap_size;
 };
 
+namespace detail {
+// Barrier over every thread of the thread-block cluster, with release /
+// acquire semantics (shared and distributed shared memory writes before it
+// are visible after it).
+__device__ inline void cluster_barrier() {
+#ifdef __CUDA_ARCH__
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+#endif
+}
+__device__ inline unsigned int cluster_ctarank() {
+  unsigned int r = 0;
+#ifdef __CUDA_ARCH__
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+#endif
+  return r;
+}
+__device__ inline unsigned int cluster_nctarank() {
+  unsigned int r = 1;
+#ifdef __CUDA_ARCH__
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+#endif
+  return r;
+}
+}  // namespace detail
+
+// A concurrent group of C concurrent groups: one thread-block cluster of C
+// CTAs, each CTA one inner group.  this_exec is the executing CTA's group
+// (its index() is the CTA's rank in the cluster), index() is the cluster's
+// index in its grid, wait() synchronises every agent of every CTA.
+template <typename InnerAgent, std::size_t inner_size, std::size_t size_>
+class concurrent_group<concurrent_group<InnerAgent, inner_size>, size_>
+    : public parallel_group<concurrent_group<InnerAgent, inner_size>, size_> {
+  typedef parallel_group<concurrent_group<InnerAgent, inner_size>, size_> super_t;
+  static_assert(size_ >= 1 && size_ <= 16, "a cluster holds 1 to 16 CTAs");
+
+ public:
+  typedef typename super_t::agent_type agent_type;
+  typedef typename super_t::size_type size_type;
+
+  __host__ __device__ concurrent_group(agent_type exec = agent_type(), size_type i = invalid_index)
+      : super_t(exec, i) {}
+
+  __device__ void wait() const { detail::cluster_barrier(); }
+  // the heap of each CTA (its dynamic shared memory)
+  __host__ __device__ size_type heap_size() const { return this->this_exec.heap_size(); }
+  // clusters of this size that run at once on the whole GPU (occupancy)
+  __host__ static size_type hardware_concurrency() { return detail::sm_count() / size_; }
+};
+
 inline __host__ __device__ concurrent_group<> con(size_t size, size_t heap_size = use_default) {
   return concurrent_group<>(static_cast<int>(size), static_cast<int>(heap_size));
 }
@@ -216,6 +270,13 @@ inline __host__ __device__ concurrent_group<agent<grainsize>, groupsize> con(siz
 
 // A view of an execution agent or group with a static upper bound on the
 // work it does (enables fully unrolled, register-resident loops).
+// A cluster of C concurrent groups (CTAs) of `inner` agents each.
+template <std::size_t C, typename InnerAgent, std::size_t S>
+inline __host__ __device__ concurrent_group<concurrent_group<InnerAgent, S>, C> cluster(
+    concurrent_group<InnerAgent, S> inner) {
+  return concurrent_group<concurrent_group<InnerAgent, S>, C>(inner);
+}
+
 template <std::size_t bound_, typename ExecutionAgent>
 class bounded : public ExecutionAgent {
  public:

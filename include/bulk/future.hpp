@@ -4,8 +4,9 @@
 // wait() blocks until the launch finished, valid() says whether the future
 // refers to a launch; a future may own the stream it was launched into (when
 // the launch was ordered after another future, bulk/detail/async.inl:52-81).
-// Errors raise std::runtime_error with the CUDA error text (the reference
-// raises thrust::system_error).
+// Errors raise thrust::system_error in thrust::cuda_category() carrying the
+// cudaError_t, as the reference does (bulk/detail/throw_on_error.hpp:33-49);
+// it derives from std::runtime_error.
 #pragma once
 
 #include <stdexcept>
@@ -13,6 +14,8 @@
 #include <utility>
 
 #include <cuda_runtime.h>
+#include <thrust/system/cuda/error.h>
+#include <thrust/system_error.h>
 
 #include "execution_policy.hpp"
 
@@ -20,7 +23,7 @@ namespace bulk {
 namespace detail {
 
 inline void throw_on_error(cudaError_t e, const char *what) {
-  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) throw thrust::system_error(e, thrust::cuda_category(), what);
 }
 
 struct future_core_access;
@@ -50,7 +53,8 @@ class future<void> {
   }
 
   void wait() const {
-    if (!valid()) throw std::runtime_error("bulk::future::wait: no launch");
+    if (!valid()) throw thrust::system_error(cudaErrorInvalidResourceHandle, thrust::cuda_category(),
+                                             "bulk::future::wait: no launch");
     detail::throw_on_error(cudaEventSynchronize(m_event), "bulk::future::wait");
   }
   bool valid() const { return m_event != 0; }

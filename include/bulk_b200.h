@@ -91,6 +91,26 @@ BK_API int bk_workspace_status(void *d_ws, size_t ws_bytes, bk_stream_t stream);
  * Waiting tiles then give up, record BK_ERR_SPIN_TIMEOUT and return. */
 BK_API int bk_debug_set_fault(int64_t skip_publish_tile, uint64_t spin_limit_ns);
 
+/* ---- launch shapes ------------------------------------------------------
+ * The device-wide algorithms size their grids (CTAs per SM) and L2 prefetch
+ * distance from a table measured on a B200 by bulk_b200/tune.py and compiled
+ * into the library, per op, element bytes (key + value bytes for the by-key
+ * ops) and size class (n < 2^16, < 2^20, < 2^24, larger).  This replaces the
+ * reference's choose_sizes / occupancy heuristics
+ * (bulk/detail/choose_sizes.inl:32-117, cuda_launch_config.hpp:240-379).
+ * bk_tune_lookup reports the shape a call of n elements would use;
+ * bk_tune_override sets a process-wide shape for one table cell
+ * (ctas_per_sm = 0 clears it), which is how the tuning procedure tries
+ * shapes.  Ops: BK_TUNE_*; ctas_per_sm at most 8 (reduce), 2 (scan,
+ * reduce_by_key), 3 (merge), 1 (sort); prefetch 0-4. */
+#define BK_TUNE_REDUCE 0
+#define BK_TUNE_SCAN 1
+#define BK_TUNE_REDUCE_BY_KEY 2
+#define BK_TUNE_MERGE 3
+#define BK_TUNE_SORT 4
+BK_API int bk_tune_lookup(int op, int elem_bytes, uint64_t n, int32_t *ctas_per_sm, int32_t *prefetch);
+BK_API int bk_tune_override(int op, int elem_bytes, int size_class, int32_t ctas_per_sm, int32_t prefetch);
+
 /* ---- reduce -------------------------------------------------------------
  * *d_out = init (+) in[0] (+) ... (+) in[n-1]; n == 0 writes init.
  * Replaces my_reduce(first, last, init, binary_op), reduce.cu:58-97, whose

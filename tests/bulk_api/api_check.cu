@@ -364,10 +364,11 @@ struct k_reduce_by_key {
   __device__ void operator()(group_t &g, const int *keys, const int *vals, int n, int *ok, int *ov, int *count) {
     auto r = bulk::reduce_by_key(g, keys, keys + n, vals, ok, ov, -1, 1000, eq_i(), plus_i());
     if (g.this_exec.index() == 0) {
-      int *k_end = cuda::std::get<0>(r);
-      int *v_end = cuda::std::get<1>(r);
-      *k_end = cuda::std::get<2>(r);  // the open run closes at the end
-      *v_end = cuda::std::get<3>(r);
+      // the result is a thrust::tuple, read the way the reference's callers do
+      int *k_end = thrust::get<0>(r);
+      int *v_end = thrust::get<1>(r);
+      *k_end = thrust::get<2>(r);  // the open run closes at the end
+      *v_end = thrust::get<3>(r);
       *count = int(k_end - ok) + 1;
     }
   }
@@ -713,6 +714,136 @@ static void agent_algorithms() {
   check("agent bounded merge_by_key values", mv.get(), wmv);
 }
 
+// ============================================================================
+// thread-block clusters: concurrent groups of CTAs, distributed shared memory
+// ============================================================================
+typedef bulk::concurrent_group<bulk::agent<1>, 128> cta128_t;
+typedef bulk::concurrent_group<cta128_t, 4> cluster4_t;
+typedef bulk::concurrent_group<bulk::agent<1>, 64> cta64_t;
+typedef bulk::concurrent_group<cta64_t, 2> cluster2_t;
+
+struct k_cluster_reduce {  // one cluster of 4 CTAs reduces the whole range
+  __device__ void operator()(cluster4_t &g, const int *data, int n, int *out, int *ranks) {
+    const int s = bulk::reduce(g, data, data + n, 7, plus_i());
+    const int rank = g.this_exec.index(), t = g.this_exec.this_exec.index();
+    if (t == 0) {
+      out[rank] = s;  // every CTA holds the same result
+      ranks[rank] = (int)bulk::detail::cluster_ctarank() + 100 * g.size();
+    }
+  }
+};
+struct k_cluster_reduce_affine {  // a non-commutative operator across the cluster
+  __device__ void operator()(cluster4_t &g, const affine *data, int n, affine *out) {
+    const affine r = bulk::reduce(g, data, data + n, affine{1u, 0u}, compose());
+    if (g.this_exec.index() == 0 && g.this_exec.this_exec.index() == 0) *out = r;
+  }
+};
+struct k_cluster_grid {  // a grid of clusters, one segment per cluster
+  __device__ void operator()(bulk::parallel_group<cluster2_t> &grid, const int *data, int seg, int *out) {
+    cluster2_t &g = grid.this_exec;
+    const int *first = data + (size_t)g.index() * seg;
+    const int s = bulk::reduce(g, first, first + seg, 0, plus_i());
+    if (g.this_exec.index() == 1 && g.this_exec.this_exec.index() == 0) out[g.index()] = s;
+  }
+};
+// CTA 0 fills its own heap, so its next block comes from CTA 1's shared
+// memory; CTA 1 checks the pattern in its own heap, then CTA 0 frees it.
+struct k_cluster_dsmem {
+  __device__ void operator()(cluster2_t &g, int *res) {
+    const int rank = g.this_exec.index(), t = g.this_exec.this_exec.index();
+    __shared__ int *s_far;
+    if (rank == 0 && t == 0) {
+      void *a = bulk::shmalloc(600);   // this CTA's heap (1024 bytes)
+      void *b = bulk::shmalloc(600);   // does not fit here: the peer's heap
+      res[0] = __isShared(a) ? 1 : 0;
+      res[1] = (!__isShared(b) && bulk::is_on_chip(b)) ? 1 : 0;
+      int *bi = static_cast<int *>(b);
+      for (int i = 0; i < 150; ++i) bi[i] = 1000 + i;
+      s_far = bi;
+      bulk::shfree(a);
+    }
+    g.wait();
+    if (rank == 1 && t == 0) {  // the block lives in this CTA's heap
+      const unsigned char *heap = bulk::detail::s_bulk_heap;
+      const int *mine = reinterpret_cast<const int *>(heap + sizeof(bulk::detail::heap_block_header));
+      int ok = 1;
+      for (int i = 0; i < 150; ++i) ok &= mine[i] == 1000 + i;
+      res[2] = ok;
+      res[3] = (int)bulk::detail::s_heap_top;
+    }
+    g.wait();
+    if (rank == 0 && t == 0) bulk::shfree(s_far);
+    g.wait();
+    if (rank == 1 && t == 0) res[4] = (int)bulk::detail::s_heap_top;  // popped: 0
+    // a collective allocation of the whole cluster: one block every CTA reaches
+    int *shared_block = static_cast<int *>(bulk::malloc(g, 64 * sizeof(int)));
+    if (rank == 1 && t < 64) shared_block[t] = 3 * t + 1;
+    g.wait();
+    if (rank == 0 && t == 0) {
+      int ok = 1;
+      for (int i = 0; i < 64; ++i) ok &= shared_block[i] == 3 * i + 1;
+      res[5] = ok;
+      res[6] = bulk::is_on_chip(shared_block) ? 1 : 0;
+    }
+    bulk::free(g, shared_block);
+  }
+};
+
+static void cluster_programs() {
+  {
+    stage("cluster reduce");
+    const int n = 100003;
+    std::vector<int> h = random_ints(n, 41, -1000, 1000);
+    dvec<int> d(h), out(4), ranks(4);
+    bulk::async(bulk::cluster<4>(bulk::con<128, 1>(4096)), k_cluster_reduce(), bulk::root, d.p, n, out.p, ranks.p)
+        .wait();
+    const int want = std::accumulate(h.begin(), h.end(), 7);
+    check("cluster group reduce (4 CTAs, every CTA's result)", out.get(), std::vector<int>(4, want));
+    check("cluster group ranks", ranks.get(), std::vector<int>{400, 401, 402, 403});
+  }
+  {
+    stage("cluster reduce affine");
+    const int n = 77777;
+    std::vector<affine> h = random_affine(n, 43);
+    dvec<affine> d(h), out(1);
+    bulk::async(bulk::cluster<4>(bulk::con<128, 1>(4096)), k_cluster_reduce_affine(), bulk::root, d.p, n, out.p)
+        .wait();
+    affine want{1u, 0u};
+    for (const affine &x : h) want = compose()(want, x);
+    check("cluster group reduce non-commutative", out.get(), std::vector<affine>{want});
+  }
+  {
+    stage("cluster grid");
+    const int clusters = 37, seg = 5001;
+    std::vector<int> h = random_ints((size_t)clusters * seg, 47, -100, 100);
+    dvec<int> d(h), out(clusters);
+    bulk::async(bulk::par(bulk::cluster<2>(bulk::con<64, 1>(2048)), clusters), k_cluster_grid(), bulk::root, d.p, seg,
+                out.p)
+        .wait();
+    std::vector<int> want(clusters);
+    for (int c = 0; c < clusters; ++c) want[c] = std::accumulate(h.begin() + (size_t)c * seg, h.begin() + (size_t)(c + 1) * seg, 0);
+    check("grid of clusters reduce", out.get(), want);
+  }
+  {
+    stage("cluster dsmem malloc");
+    dvec<int> res(7);
+    res.put(std::vector<int>(7, -1));
+    bulk::async(bulk::cluster<2>(bulk::con<64, 1>(1024)), k_cluster_dsmem(), bulk::root, res.p).wait();
+    check("cluster heap: local block, then a block in the peer CTA's shared memory (DSMEM)", res.get(),
+          std::vector<int>{1, 1, 1, 624, 0, 1, 1});
+  }
+  {
+    stage("errors raise thrust::system_error");
+    bool caught = false;
+    try {
+      bulk::async(bulk::con(2048), sum(), bulk::root, (const int *)nullptr, 0, (int *)nullptr).wait();
+    } catch (const thrust::system_error &e) {
+      caught = e.code().value() != 0;
+    }
+    check_true("errors raise thrust::system_error", caught);
+  }
+}
+
 int main(int argc, char **argv) {
   std::setvbuf(stdout, nullptr, _IONBF, 0);
   const std::string only = argc > 1 ? argv[1] : "";
@@ -725,6 +856,7 @@ int main(int argc, char **argv) {
   if (only.empty() || only == "drivers") driver_programs();
   if (only.empty() || only == "group") group_algorithms();
   if (only.empty() || only == "agent") agent_algorithms();
+  if (only.empty() || only == "cluster") cluster_programs();
   CUDA_OK(cudaDeviceSynchronize());
   std::printf("%s: %d failure(s)\n", g_failures ? "FAILED" : "PASSED", g_failures);
   return g_failures ? 1 : 0;

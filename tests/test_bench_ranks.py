@@ -67,11 +67,27 @@ def test_reference_arm_runs_on_rank_zero_only():
 
 
 def test_reference_arm_line_keeps_the_contract():
-    """Rank 0's line (a tiny sample: the real arm sizes its own)."""
+    """Rank 0's line, on a small n here (the real arm runs the 2^28 workload)."""
     sys.path.insert(0, str(ROOT))
     import bench
-    line = bench.cpu_reference_line(1, 1)
+    line = bench.cpu_reference_line(1, 1, n=1 << 20)
     json.dumps(line)
     assert line["impl"] == "reference" and line["unit"] == "GB/s" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+
+
+def test_cpu_baseline_object_reports_all_cores_and_one_thread(monkeypatch):
+    sys.path.insert(0, str(ROOT))
+    import bench
+    calls = []
+
+    def fake(n, steps, warmup, threads):
+        calls.append((n, threads))
+        return 0.5, "reference", steps
+    monkeypatch.setattr(bench, "cpu_reference_time", fake)
+    cb = bench.cpu_baseline_object()
+    assert cb["cores"] == (os.cpu_count() or 1) and cb["one_thread"]["cores"] == 1
+    assert calls == [(1 << 26, os.cpu_count() or 1), (1 << 24, 1)]
+    # bytes per element: reduce N*s + scan 2*N*s for s = 4, 8, 4
+    assert cb["value"] == 48 * (1 << 26) / 0.5 / 1e9 and cb["cpu_model"]

@@ -66,5 +66,7 @@ def test_api_program_runs(api_binary):
                  "scatter_if", "for_each_n", "adjacent_difference", "strided_iterator", "group merge na=",
                  "merge_by_key", "inplace_merge", "stable_sort_by_key", "group stable_sort n=",
                  "group reduce_by_key", "group malloc", "uninitialized", "agent bounded reduce",
-                 "agent bounded merge_by_key"]:
+                 "agent bounded merge_by_key", "cluster group reduce (4 CTAs", "cluster group reduce non-commutative",
+                 "grid of clusters reduce", "block in the peer CTA's shared memory (DSMEM)",
+                 "errors raise thrust::system_error"]:
         assert name in text, name
