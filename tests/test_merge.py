@@ -102,3 +102,6 @@ def test_full_size_config_2x2_26_f32_u32(cuda):
     nondecreasing = (kk[1:] > kk[:-1]) | ((kk[1:] == kk[:-1]) & (v[1:] > v[:-1]))
     assert bool(nondecreasing.all())
     assert int(from_a.sum()) == n
+    # and element by element against the oracle's stable merge
+    wk, wv = oracle.merge(a, b, np.arange(n, dtype=np.uint32), np.arange(n, 2 * n, dtype=np.uint32))
+    assert np.array_equal(host(k), wk) and np.array_equal(host(v).view(np.uint32), wv)

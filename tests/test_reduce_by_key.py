@@ -66,7 +66,10 @@ def _vals(tag, n, seed):
 
 @pytest.mark.parametrize("kt,vt", COMBOS)
 def test_edge_sizes_and_run_shapes(cuda, kt, vt):
-    for i, n in enumerate([0, 1, 2, 3, 4095, 4096, 4097, 8192, 2 * 4096 + 1, 100003]):
+    # 2064, 4128, 12384: a last tile whose rows the tensor copies still cover
+    # (or, for 8-byte values, whose key rows they do not), next to the sizes
+    # whose ragged end is staged by plain loads
+    for i, n in enumerate([0, 1, 2, 3, 2064, 4095, 4096, 4097, 4128, 8192, 2 * 4096 + 1, 12384, 100003]):
         for kind in ("geometric", "distinct", "one"):
             keys = _runs(kind, n, 5 + i).astype(NP[kt])
             vals = _vals(vt, n, 7 + i)

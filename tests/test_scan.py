@@ -94,12 +94,15 @@ def test_stuck_predecessor_times_out_with_an_error(cuda):
 @pytest.mark.parametrize("tag", ["i32", "f32", "f64"])
 def test_full_size_2_28(cuda, tag):
     n = 1 << 28
-    x = dev(gen(tag, n, 0))
+    xh = gen(tag, n, 0)
+    x = dev(xh)
     out = bulk_b200.inclusive_scan(x, NP[tag](0))
     if tag == "i32":
         # size-independent properties: first element and adjacent differences
         assert out[0].item() == x[0].item()
         assert torch.equal(out[1:] - out[:-1], x[1:])
+        # and element by element against the oracle (exact, wrapping)
+        assert np.array_equal(host(out), oracle.inclusive_scan(xh, np.int32(0)))
     else:
         ref = torch.cumsum(x.double(), 0)
         mag = torch.cumsum(x.double().abs(), 0)

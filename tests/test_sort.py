@@ -100,6 +100,9 @@ def test_full_size_2_26_payload_is_index(cuda, tag):
     assert bool(ok.all())
     assert torch.equal(torch.sort(vals).values, torch.arange(n, dtype=torch.int32, device=cuda))
     assert torch.equal(ks, k0[vals.long()])
+    # and element by element against the oracle's stable sort
+    wk, wv = oracle.stable_sort_by_key(host(keys0), np.arange(n, dtype=np.uint32))
+    assert np.array_equal(host(keys), wk) and np.array_equal(host(vals).view(np.uint32), wv)
 
 
 @pytest.mark.parametrize("tag", ["f32", "f64"])
