@@ -95,6 +95,18 @@ __device__ __forceinline__ void tma_load_rows(void *smem_dst, const CUtensorMap 
       : "memory");
 }
 
+// Tiled 2-D copy shared -> global of a box at row `row` of the row view
+// `map`, tracked by the issuing thread's bulk group (rows past the view are
+// not written).
+__device__ __forceinline__ void tma_store_rows(const CUtensorMap *map, uint32_t row, const void *smem_src,
+                                               uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%1, %2}], [%3], %4;" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(0), "r"(row), "r"(smem_addr(smem_src)), "l"(policy)
+      : "memory");
+}
+
 // Byte offset at which a tensor copy with the 128-byte swizzle places byte
 // `o` of a 1024-byte-aligned box of 128-byte rows: the 16-byte chunk index
 // within each row is XORed with the row index mod 8, so eight lanes that

@@ -117,18 +117,6 @@ __device__ __forceinline__ void merge_load_range(T *dst, const T *src, uint64_t 
   for (uint64_t i = bulk_hi > lo ? bulk_hi : lo; i < hi; ++i) dst[i - lo] = src[i];
 }
 
-// Tiled 2-D copy shared -> global of a box at row `row` of the row view
-// `map`, tracked by the issuing thread's bulk group (rows past the view are
-// not written).
-__device__ __forceinline__ void tma_store_rows(const CUtensorMap *map, uint32_t row, const void *smem_src,
-                                               uint64_t policy) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%1, %2}], [%3], %4;" ::"l"(
-          reinterpret_cast<uint64_t>(map)),
-      "r"(0), "r"(row), "r"(smem_addr(smem_src)), "l"(policy)
-      : "memory");
-}
-
 // Persistent merge.  Warps 0-7 merge; warp 8's lane 0 loads and stores.
 // CTA c takes tiles c, c + G, c + 2G, ... (G = gridDim.x); tile i of the CTA
 // uses buffer i mod 2 and goes through:

@@ -71,25 +71,39 @@ struct ScanTile {
   T *out;          // its first output element
   uint32_t count;  // elements in the tile
   bool first;      // first tile of its array: publishes its inclusive prefix at once
-  bool tma;        // in and out 16-byte aligned
+  bool tma;        // moved by TMA copies (in and out 16-byte aligned; in the
+                   // blocked layout also inside whole rows of both row views)
   T init;          // its array's init
+  uint32_t index;  // tile index within its array
 };
 
-// Tile source: one array.
+// Tile source: one array.  For 8-byte elements (kSwz) tiles move by tiled
+// tensor copies of 128-byte rows with the 128-byte swizzle, and each lane
+// owns 16 consecutive elements (the "blocked" layout: one lane-local scan and
+// one warp scan per 16 elements, where the row layout needs a warp scan for
+// every 2), read and written conflict-free; tiles past `covered` (the ragged
+// end) are read and written by the compute warps directly.  4-byte elements
+// keep the row layout (rows of 32 lanes x 16 bytes) and untiled bulk copies.
 template <typename T>
 struct ScanOne {
+  static constexpr bool kSwz = sizeof(T) == 8;
+  CUtensorMap imap;  // input as rows of 128 bytes (kSwz)
+  CUtensorMap omap;  // output as rows of 128 bytes (kSwz)
   const T *in;
   T *out;
   uint64_t n;
   T init;
-  int tma;
+  int tma;           // in and out 16-byte aligned
+  uint64_t covered;  // kSwz: leading elements inside whole rows of both views
   __device__ __forceinline__ ScanTile<T> tile(unsigned int t) const {
     const uint64_t base = (uint64_t)t * ScanCfg<T>::TILE;
     const uint64_t rem = n - base;
-    return ScanTile<T>{in + base, out + base,
-                       (uint32_t)(rem < (uint64_t)ScanCfg<T>::TILE ? rem : (uint64_t)ScanCfg<T>::TILE), t == 0u,
-                       tma != 0, init};
+    const uint32_t cnt = (uint32_t)(rem < (uint64_t)ScanCfg<T>::TILE ? rem : (uint64_t)ScanCfg<T>::TILE);
+    const bool t_tma = kSwz ? (base + cnt <= covered) : (tma != 0);
+    return ScanTile<T>{in + base, out + base, cnt, t == 0u, t_tma, init, t};
   }
+  __device__ __forceinline__ const CUtensorMap *in_map() const { return &imap; }
+  __device__ __forceinline__ const CUtensorMap *out_map() const { return &omap; }
 };
 
 // Tile source: a batch of independent arrays scanned by one launch.  Array
@@ -99,6 +113,7 @@ struct ScanOne {
 constexpr int kScanBatchMax = 256;
 template <typename T>
 struct ScanBatch {
+  static constexpr bool kSwz = false;
   const T *in[kScanBatchMax];
   T *out[kScanBatchMax];
   uint64_t n[kScanBatchMax];
@@ -118,23 +133,59 @@ struct ScanBatch {
     const bool tma = ((reinterpret_cast<uintptr_t>(in[lo]) | reinterpret_cast<uintptr_t>(out[lo])) & 15) == 0;
     return ScanTile<T>{in[lo] + base, out[lo] + base,
                        (uint32_t)(rem < (uint64_t)ScanCfg<T>::TILE ? rem : (uint64_t)ScanCfg<T>::TILE),
-                       local == 0u, tma, init[lo]};
+                       local == 0u, tma, init[lo], local};
   }
+  __device__ __forceinline__ const CUtensorMap *in_map() const { return nullptr; }
+  __device__ __forceinline__ const CUtensorMap *out_map() const { return nullptr; }
 };
 
 // Copies a tile into shared memory `buf`: the 16-byte-aligned body with one
 // TMA bulk copy completing on `bar` (returns whether one was issued), the
 // ragged tail (fewer than V elements) with plain loads by the calling thread.
 // Called by one thread, only for tiles whose pointers are 16-byte aligned.
-template <typename T>
-__device__ __forceinline__ bool scan_issue_tile_load(const ScanTile<T> &tl, T *buf, uint64_t *bar, uint64_t policy) {
+template <typename T, typename Src>
+__device__ __forceinline__ bool scan_issue_tile_load(const Src &src, const ScanTile<T> &tl, T *buf, uint64_t *bar,
+                                                     uint64_t policy) {
   using C = ScanCfg<T>;
+  if constexpr (Src::kSwz) {  // blocked layout: the tile's rows, swizzled (a TMA tile is whole rows)
+    mbar_arrive_expect_tx(bar, (uint32_t)C::TILE_BYTES);
+    tma_load_rows(buf, src.in_map(), tl.index * (uint32_t)(C::TILE_BYTES / 128), bar, policy);
+    return true;
+  }
   const uint32_t bulk = tl.count & ~(uint32_t)(C::V - 1);
   for (uint32_t i = bulk; i < tl.count; ++i) buf[i] = tl.in[i];
   if (bulk == 0) return false;
   mbar_arrive_expect_tx(bar, bulk * (uint32_t)sizeof(T));
   tma_load_1d_hint(buf, tl.in, bulk * (uint32_t)sizeof(T), bar, policy);
   return true;
+}
+
+// Blocked layout (8-byte elements): compute lane li = warp * 32 + lane owns
+// elements [li * M, li * M + M) of its tile, M = 16 (one 128-byte row); in a
+// swizzled buffer its 16-byte chunk c sits at swz128(li * 128 + 16 c).
+// Loads a lane's elements (elements past the tile's end read as identity);
+// tiles without a TMA copy are read from global memory directly.
+template <typename T, typename Op>
+__device__ __forceinline__ void scan_blk_load(const ScanTile<T> &tl, const T *buf, uint32_t li,
+                                              T (&x)[ScanCfg<T>::TILE / (32 * kScanWarps)]) {
+  constexpr int M = ScanCfg<T>::TILE / (32 * kScanWarps), VC = 16 / sizeof(T);
+  const uint32_t e0 = li * M;
+  if (tl.tma) {
+    const unsigned char *b = reinterpret_cast<const unsigned char *>(buf);
+#pragma unroll
+    for (int c = 0; c < M / VC; ++c) {
+      const uint4 q = *reinterpret_cast<const uint4 *>(b + swz128(e0 * (uint32_t)sizeof(T) + 16u * c));
+      memcpy(&x[c * VC], &q, 16);
+    }
+    if (tl.count < (uint32_t)ScanCfg<T>::TILE) {
+#pragma unroll
+      for (int j = 0; j < M; ++j)
+        if (e0 + j >= tl.count) x[j] = Op::identity();
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < M; ++j) x[j] = (e0 + j < tl.count) ? tl.in[e0 + j] : Op::identity();
+  }
 }
 
 // Persistent two-phase scan.  Warps 0-7 compute, warp 8 (lane 0) loads and
@@ -182,8 +233,10 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
   constexpr int V = C::V, TILE = C::TILE, R = kScanRowsPerWarp, NB = kScanBufs, Q = kScanQueue;
   constexpr unsigned int NONE = 0xffffffffu;
   Op op;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  T *const buf0 = reinterpret_cast<T *>(smem_raw);  // NB tile buffers
+  constexpr bool BLK = Src::kSwz;
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  // NB tile buffers from the first 1024-byte boundary (the swizzle's period)
+  T *const buf0 = reinterpret_cast<T *>(smem_dyn + ((1024u - (smem_addr(smem_dyn) & 1023u)) & 1023u));
   __shared__ __align__(8) uint64_t s_full[NB];
   __shared__ __align__(8) uint64_t s_p1[NB];
   __shared__ __align__(8) uint64_t s_p2[NB];
@@ -197,20 +250,12 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
   __shared__ unsigned int s_q_in;        // entries queued
   __shared__ int s_abort;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // a TMA copy exists for `tile` exactly when this holds (scan_issue_tile_load)
-  auto has_tma = [&](unsigned int tile) -> bool {
-    if (tile == NONE) return false;
-    const ScanTile<T> tl = src.tile(tile);
-    return tl.tma && (tl.count & ~(uint32_t)(V - 1)) != 0u;
-  };
   auto abort_now = [&]() { *reinterpret_cast<volatile int *>(&s_abort) = 1; };
   auto aborted = [&]() -> bool { return *reinterpret_cast<volatile int *>(&s_abort) != 0; };
   auto buf = [&](int b) { return buf0 + b * TILE; };
 
   uint64_t keep = 0, stream = 0;
-  uint32_t armed[NB];  // loader: phases armed on s_full[b]
-#pragma unroll
-  for (int b = 0; b < NB; ++b) armed[b] = 0u;
+  uint32_t armpar = 0u, armany = 0u;  // loader: parity of the phases armed on s_full[b] / any armed
   unsigned int next_raw = NONE;  // loader: next ticket, not yet range-checked
   unsigned int t_first = NONE;   // loader: t_0
   if (tid == 32 * kScanWarps) {
@@ -231,14 +276,15 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
     bool tx = false;
     if (t_first != NONE) {
       const ScanTile<T> tl = src.tile(t_first);
-      if (tl.tma) tx = scan_issue_tile_load(tl, buf(0), &s_full[0], keep);
+      if (tl.tma) tx = scan_issue_tile_load(src, tl, buf(0), &s_full[0], keep);
     }
     if (!tx) mbar_arrive(&s_full[0]);
-    armed[0] = 1u;
+    armpar |= 1u;
     // iteration 0's phase 2 reads buffer NB - 1, which no re-read filled:
     // give it an empty phase
     mbar_arrive(&s_full[NB - 1]);
-    armed[NB - 1] = 1u;
+    armpar |= 1u << (NB - 1);
+    armany = armpar;
     if (t_first != NONE) next_raw = atomicAdd(&hdr->tile_ticket, 1u);
   }
   __syncthreads();
@@ -246,9 +292,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
   if (warp == kScanWarps) {
     // ================= the loader (lane 0) =================
     if (lane != 0) return;
-    uint32_t p1par[NB], p2par[NB];
-#pragma unroll
-    for (int b = 0; b < NB; ++b) p1par[b] = p2par[b] = 0u;
+    uint32_t p1par = 0u, p2par = 0u;  // bit b: parity of the next phase of s_p1[b] / s_p2[b]
     bool issued_store = false;
     unsigned int t = t_first, p_tile = NONE, q_tile = NONE;
     for (int it = 0;; ++it) {
@@ -262,11 +306,12 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
         const ScanTile<T> tl = src.tile(tn);
         if (tl.tma) {
           if (issued_store) tma_store_wait_read();
-          tx = scan_issue_tile_load(tl, buf(bn), &s_full[bn], keep);
+          tx = scan_issue_tile_load(src, tl, buf(bn), &s_full[bn], keep);
         }
       }
       if (!tx) mbar_arrive(&s_full[bn]);
-      ++armed[bn];
+      armpar ^= 1u << bn;
+      armany |= 1u << bn;
       next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
       // tiles are ticketed about in order, gridDim.x per iteration: ask L2
       // now for the one some CTA will load an iteration from now
@@ -276,30 +321,35 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       }
       // once the compute warps are done with buffer bt (phase 1 of t, or
       // just its empty phase), re-read t_{i-1} from L2 into it
-      if (!mbar_wait_or_abort(&s_p1[bt], p1par[bt], spin_limit_ns, &s_abort)) {
+      if (!mbar_wait_or_abort(&s_p1[bt], (p1par >> bt) & 1u, spin_limit_ns, &s_abort)) {
         record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
         abort_now();
         break;
       }
-      p1par[bt] ^= 1u;
+      p1par ^= 1u << bt;
       tx = false;
       if (q_tile != NONE) {
         const ScanTile<T> tl = src.tile(q_tile);
-        if (tl.tma) tx = scan_issue_tile_load(tl, buf(bt), &s_full[bt], stream);
+        if (tl.tma) tx = scan_issue_tile_load(src, tl, buf(bt), &s_full[bt], stream);
       }
       if (!tx) mbar_arrive(&s_full[bt]);
-      ++armed[bt];
+      armpar ^= 1u << bt;
+      armany |= 1u << bt;
       // once the compute warps are done with buffer bp (phase 2 of p, or just
       // its empty phase), store p; the buffer then takes the next prefetch
-      if (!mbar_wait_or_abort(&s_p2[bp], p2par[bp], spin_limit_ns, &s_abort)) {
+      if (!mbar_wait_or_abort(&s_p2[bp], (p2par >> bp) & 1u, spin_limit_ns, &s_abort)) {
         record_error(hdr, BK_ERR_SPIN_TIMEOUT, p);
         abort_now();
         break;
       }
-      p2par[bp] ^= 1u;
+      p2par ^= 1u << bp;
       if (p != NONE) {
         const ScanTile<T> tl = src.tile(p);
-        if (tl.tma) {
+        if (BLK && tl.tma) {  // whole rows: the tensor store undoes the swizzle
+          tma_store_rows(src.out_map(), tl.index * (uint32_t)(C::TILE_BYTES / 128), buf(bp), stream);
+          tma_store_commit();
+          issued_store = true;
+        } else if (tl.tma) {
           const T *bP = buf(bp);
           const uint32_t bulk = tl.count & ~(uint32_t)(V - 1);
           if (bulk > 0) {
@@ -321,7 +371,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
     // a phase that already completed returns at once.
     if (issued_store) tma_store_wait_all();
     for (int b = 0; b < NB; ++b)
-      if (armed[b] != 0u) (void)mbar_wait(&s_full[b], (armed[b] - 1u) & 1u, spin_limit_ns);
+      if ((armany >> b) & 1u) (void)mbar_wait(&s_full[b], ((armpar >> b) & 1u) ^ 1u, spin_limit_ns);
     return;
   }
 
@@ -381,9 +431,7 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
   }
 
   // ================= the compute warps =================
-  uint32_t fpar[NB];
-#pragma unroll
-  for (int b = 0; b < NB; ++b) fpar[b] = 0u;
+  uint32_t fpar = 0u;  // bit b: parity of the next phase of s_full[b]
   unsigned int p_tile = NONE, q_tile = NONE;  // t_{i-2}, t_{i-1}
   bool bad = false;                           // this thread saw a failure
 
@@ -393,8 +441,8 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
 
     // ---- phase 1 of t: wait for buffer bt, learn t
     unsigned int t = NONE;
-    if (!mbar_wait_or_abort(&s_full[bt], fpar[bt], spin_limit_ns, &s_abort)) bad = true;
-    fpar[bt] ^= 1u;
+    if (!mbar_wait_or_abort(&s_full[bt], (fpar >> bt) & 1u, spin_limit_ns, &s_abort)) bad = true;
+    fpar ^= 1u << bt;
     bad = __any_sync(0xffffffffu, bad);  // warp-uniform, so the shuffles below never diverge
     if (!bad) t = s_ticket[bt];
     if (t != NONE) {
@@ -402,7 +450,13 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       const uint32_t count = tl.count;
       const T *bT = buf(bt);
       T a = Op::identity();
-      if (tl.tma && count == (uint32_t)C::TILE) {
+      if constexpr (BLK) {
+        constexpr int M = C::TILE / (32 * kScanWarps);
+        T x[M];
+        scan_blk_load<T, Op>(tl, bT, (uint32_t)(warp * 32 + lane), x);
+#pragma unroll
+        for (int j = 0; j < M; ++j) a = op(a, x[j]);
+      } else if (tl.tma && count == (uint32_t)C::TILE) {
         // a full tile in shared memory: no element is past its end
 #pragma unroll
         for (int k = 0; k < R; ++k) {
@@ -463,8 +517,8 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
     }
 
     // ---- phase 2 of p: buffer bp (re-read last iteration), prefix = queue entry it - 2
-    if (!mbar_wait_or_abort(&s_full[bp], fpar[bp], spin_limit_ns, &s_abort)) bad = true;
-    fpar[bp] ^= 1u;
+    if (!mbar_wait_or_abort(&s_full[bp], (fpar >> bp) & 1u, spin_limit_ns, &s_abort)) bad = true;
+    fpar ^= 1u << bp;
     if (p != NONE && !bad) {
       const unsigned int e = (unsigned int)it - 2u;
       if (!mbar_wait_or_abort(&s_qbar[e % Q], (e / Q) & 1u, spin_limit_ns, &s_abort)) bad = true;
@@ -477,59 +531,87 @@ __global__ void __launch_bounds__(kScanThreads, 2) scan_kernel(const __grid_cons
       const unsigned int e = (unsigned int)it - 2u;
       // everything before this warp's first element
       T before = warp == 0 ? s_q_prefix[e % Q] : op(s_q_prefix[e % Q], s_wexcl[(it + 2) & 3][warp]);
-      T y[R][V], incl[R];
+      if constexpr (BLK) {
+        constexpr int M = C::TILE / (32 * kScanWarps), VC = 16 / sizeof(T);
+        const uint32_t li = (uint32_t)(warp * 32 + lane), e0 = li * M;
+        T y[M];
+        scan_blk_load<T, Op>(tl, bP, li, y);
 #pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
-        if (tl.tma) {
-          const uint4 c = reinterpret_cast<const uint4 *>(bP)[elem / V];
-          memcpy(&y[k][0], &c, 16);
-        } else {
-#pragma unroll
-          for (int j = 0; j < V; ++j) y[k][j] = (elem + j < count) ? tl.in[elem + j] : Op::identity();
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
-        if (elem + V > count) {
-#pragma unroll
-          for (int j = 0; j < V; ++j)
-            if (elem + j >= count) y[k][j] = Op::identity();
-        }
-#pragma unroll
-        for (int j = 1; j < V; ++j) y[k][j] = op(y[k][j - 1], y[k][j]);
-        incl[k] = y[k][V - 1];
-      }
-      // the rows' warp scans, interleaved so their shuffle chains overlap
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const T o = shfl_up(incl[k], d);
-          if (lane >= d) incl[k] = op(o, incl[k]);
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const T ex = shfl_up(incl[k], 1);
-        const T tot = shfl_idx_any(incl[k], 31);
+        for (int j = 1; j < M; ++j) y[j] = op(y[j - 1], y[j]);
+        const T incl = warp_inclusive_scan(y[M - 1], op, lane);
+        const T ex = shfl_up(incl, 1);
         const T b = lane != 0 ? op(before, ex) : before;
 #pragma unroll
-        for (int j = 0; j < V; ++j) y[k][j] = op(b, y[k][j]);
-        before = op(before, tot);
-        const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+        for (int j = 0; j < M; ++j) y[j] = op(b, y[j]);
         if (tl.tma) {
-          uint4 c;
-          memcpy(&c, &y[k][0], 16);
-          reinterpret_cast<uint4 *>(bP)[elem / V] = c;
+          unsigned char *bb = reinterpret_cast<unsigned char *>(bP);
+#pragma unroll
+          for (int c = 0; c < M / VC; ++c) {
+            uint4 q;
+            memcpy(&q, &y[c * VC], 16);
+            *reinterpret_cast<uint4 *>(bb + swz128(e0 * (uint32_t)sizeof(T) + 16u * c)) = q;
+          }
+          fence_proxy_async_smem();  // the tensor store reads what this thread wrote
         } else {
 #pragma unroll
-          for (int j = 0; j < V; ++j)
-            if (elem + j < count) tl.out[elem + j] = y[k][j];
+          for (int j = 0; j < M; ++j)
+            if (e0 + j < count) tl.out[e0 + j] = y[j];
         }
+      } else {
+        T y[R][V], incl[R];
+  #pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+          if (tl.tma) {
+            const uint4 c = reinterpret_cast<const uint4 *>(bP)[elem / V];
+            memcpy(&y[k][0], &c, 16);
+          } else {
+  #pragma unroll
+            for (int j = 0; j < V; ++j) y[k][j] = (elem + j < count) ? tl.in[elem + j] : Op::identity();
+          }
+        }
+  #pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+          if (elem + V > count) {
+  #pragma unroll
+            for (int j = 0; j < V; ++j)
+              if (elem + j >= count) y[k][j] = Op::identity();
+          }
+  #pragma unroll
+          for (int j = 1; j < V; ++j) y[k][j] = op(y[k][j - 1], y[k][j]);
+          incl[k] = y[k][V - 1];
+        }
+        // the rows' warp scans, interleaved so their shuffle chains overlap
+  #pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+  #pragma unroll
+          for (int k = 0; k < R; ++k) {
+            const T o = shfl_up(incl[k], d);
+            if (lane >= d) incl[k] = op(o, incl[k]);
+          }
+        }
+  #pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const T ex = shfl_up(incl[k], 1);
+          const T tot = shfl_idx_any(incl[k], 31);
+          const T b = lane != 0 ? op(before, ex) : before;
+  #pragma unroll
+          for (int j = 0; j < V; ++j) y[k][j] = op(b, y[k][j]);
+          before = op(before, tot);
+          const uint32_t elem = (uint32_t)(((warp * R + k) * 32 + lane) * V);
+          if (tl.tma) {
+            uint4 c;
+            memcpy(&c, &y[k][0], 16);
+            reinterpret_cast<uint4 *>(bP)[elem / V] = c;
+          } else {
+  #pragma unroll
+            for (int j = 0; j < V; ++j)
+              if (elem + j < count) tl.out[elem + j] = y[k][j];
+          }
+        }
+        if (tl.tma) fence_proxy_async_smem();
       }
-      if (tl.tma) fence_proxy_async_smem();
     }
     __syncwarp();
     if (!bad && lane == 0) mbar_arrive(&s_p2[bp]);
@@ -559,7 +641,7 @@ int scan_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStre
   if (st != BK_OK) return st;
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
-  const size_t smem = (size_t)kScanBufs * C::TILE_BYTES;
+  const size_t smem = (size_t)kScanBufs * C::TILE_BYTES + 1024;  // + room to align the buffers to 1024 bytes
   struct Site {};
   host::KernelSetup ks;
   if ((st = host::kernel_setup<Site>(scan_kernel<T, Op, Src>, kScanThreads, smem, &ks)) != BK_OK) return st;
@@ -580,7 +662,22 @@ int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t 
   if (d_in == nullptr || d_out == nullptr) return BK_ERR_INVALID_ARGUMENT;
   if (!host::aligned_to<T>(d_in) || !host::aligned_to<T>(d_out)) return BK_ERR_MISALIGNED;
   const int tma = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15) == 0;
-  const ScanOne<T> src{d_in, d_out, n, init, tma};
+  ScanOne<T> src;
+  memset(&src, 0, sizeof(src));
+  src.in = d_in;
+  src.out = d_out;
+  src.n = n;
+  src.init = init;
+  src.tma = tma;
+  if constexpr (ScanOne<T>::kSwz) {
+    // row views of the input and output: the tiles inside whole 128-byte rows
+    // of both move by tensor copies, the ragged end by plain loads and stores
+    constexpr uint32_t box_rows = (uint32_t)(ScanCfg<T>::TILE_BYTES / 128);
+    const uint64_t rows = n * sizeof(T) / 128;
+    if (tma && rows > 0 && host::encode_rows_128b(&src.imap, d_in, rows, box_rows) == BK_OK &&
+        host::encode_rows_128b(&src.omap, d_out, rows, box_rows) == BK_OK)
+      src.covered = rows * (128 / sizeof(T));
+  }
   return scan_run<T, Op>(src, scan_num_tiles<T>(n), d_ws, ws_bytes, stream);
 }
 
