@@ -3,13 +3,16 @@
 For each op, element size and size class, every candidate shape is set
 through bk_tune_override, the op is timed on one B200 with CUDA events
 (median of 5 after 2 warm-up calls; a size class is represented by one n:
-2^15, 2^19, 2^23 and 2^26 elements), and the fastest shape is kept.  The
+2^15, 2^19, 2^23 and 2^26 elements), and the fastest shape is kept when it
+beats the op's default shape by more than 3 % (otherwise the default stays:
+smaller differences are run-to-run noise).  The
 table and the timings behind it go to bulk_b200/csrc/tuning_table.inc (C++
 initialisers, compiled into libbulkb200.so) and bulk_b200/tuning_table.json
 (provenance: device, date, every candidate's time).  Rebuild the library
 afterwards (python bulk_b200/build.py).
 
 Usage (on a GPU machine): python bulk_b200/tune.py [--quick]
+        python bulk_b200/tune.py --from-json   (rewrite the .inc from the recorded timings)
 """
 from __future__ import annotations
 
@@ -26,6 +29,18 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 OPS = {"reduce": 0, "scan": 1, "reduce_by_key": 2, "merge": 3, "sort": 4}
+# the library's defaults (bk_tune.hpp default_knobs)
+DEFAULT = {"reduce": (4, 0), "scan": (2, 0), "reduce_by_key": (2, 0), "merge": (3, 0), "sort": (1, 1)}
+MARGIN = 0.03
+
+
+def choose(op, res):
+    """The fastest shape if it beats the default by more than MARGIN, else the default."""
+    best = min(res, key=lambda r: r[1])
+    dflt = [t for shape, t in res if shape == DEFAULT[op]]
+    if dflt and best[1] > dflt[0] * (1.0 - MARGIN):
+        return DEFAULT[op]
+    return best[0]
 CLASS_N = [1 << 15, 1 << 19, 1 << 23, 1 << 26]
 # (op, label, element bytes, candidate (ctas_per_sm, prefetch) shapes)
 PLAN = [
@@ -121,36 +136,63 @@ def tune(quick=False):
                 _lib.check(lib.bk_tune_override(OPS[op], eb, sc, c, pf), "bk_tune_override")
                 res.append(((c, pf), _time(op, d, 5, inner)))
             _lib.check(lib.bk_tune_override(OPS[op], eb, sc, 0, 0), "bk_tune_override")
-            best = min(res, key=lambda r: r[1])
-            entries.append((OPS[op], eb, sc, best[0]))
+            best = choose(op, res)
+            entries.append((OPS[op], eb, sc, best))
             record.append({"op": op, "dtype": label, "elem_bytes": eb, "size_class": sc, "n": n,
                            "candidates_ms": {f"ctas{c}_pf{pf}": t for (c, pf), t in res},
-                           "chosen": {"ctas_per_sm": best[0][0], "prefetch": best[0][1]}})
+                           "chosen": {"ctas_per_sm": best[0], "prefetch": best[1]}})
             print(f"{op:14s} {label:8s} n=2^{n.bit_length() - 1:<2d} " +
-                  " ".join(f"{c}/{pf}:{t:.4f}" for (c, pf), t in res) + f"  -> {best[0]}", flush=True)
+                  " ".join(f"{c}/{pf}:{t:.4f}" for (c, pf), t in res) + f"  -> {best}", flush=True)
             del d
             torch.cuda.empty_cache()
     props = torch.cuda.get_device_properties(dev)
     prov = {"device": props.name, "sms": props.multi_processor_count,
             "date_utc": time.strftime("%Y-%m-%d %H:%M", time.gmtime()),
-            "procedure": "bulk_b200/tune.py: median of 5 timed calls (CUDA events) after 2 warm-up calls per shape",
+            "procedure": ("bulk_b200/tune.py: median of 5 timed calls (CUDA events) after 2 warm-up calls per "
+                          f"shape; the default shape stays unless another is more than {MARGIN:.0%} faster"),
             "cells": record}
+    write_table(prov, entries)
+    return entries
+
+
+def write_table(prov, entries):
     names = {v: k for k, v in OPS.items()}
     lines = ["// Launch-shape table: {op, element bytes, size class, {ctas_per_sm, prefetch}}.",
-             f"// Measured by bulk_b200/tune.py on {props.name} ({props.multi_processor_count} SMs), "
+             f"// Measured by bulk_b200/tune.py on {prov['device']} ({prov['sms']} SMs), "
              f"{prov['date_utc']} UTC; timings in bulk_b200/tuning_table.json."]
     for op, eb, sc, (c, pf) in entries:
         lines.append(f"{{bk::tune::k{''.join(w.capitalize() for w in names[op].split('_'))}, {eb}, {sc}, {{{c}, {pf}}}}},")
     (PKG / "csrc" / "tuning_table.inc").write_text("\n".join(lines) + "\n")
     (PKG / "tuning_table.json").write_text(json.dumps(prov, indent=1) + "\n")
+
+
+def from_json():
+    """Re-choose every cell from the recorded candidate timings and rewrite both files."""
+    prov = json.loads((PKG / "tuning_table.json").read_text())
+    entries = []
+    for cell in prov["cells"]:
+        res = []
+        for key, t in cell["candidates_ms"].items():
+            c, pf = key.replace("ctas", "").split("_pf")
+            res.append(((int(c), int(pf)), t))
+        best = choose(cell["op"], res)
+        cell["chosen"] = {"ctas_per_sm": best[0], "prefetch": best[1]}
+        entries.append((OPS[cell["op"]], cell["elem_bytes"], cell["size_class"], best))
+    prov["procedure"] = ("bulk_b200/tune.py: median of 5 timed calls (CUDA events) after 2 warm-up calls per "
+                         f"shape; the default shape stays unless another is more than {MARGIN:.0%} faster")
+    write_table(prov, entries)
     return entries
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--quick", action="store_true", help="the largest size class only")
+    ap.add_argument("--from-json", action="store_true", help="rewrite the table from the recorded timings")
     a = ap.parse_args(argv)
-    tune(a.quick)
+    if a.from_json:
+        from_json()
+    else:
+        tune(a.quick)
     return 0
 
 
