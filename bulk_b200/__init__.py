@@ -24,6 +24,7 @@ from .batch import (  # noqa: F401
     inclusive_scan_batch,
     reduce_by_key_batch,
     stable_sort_by_key_batch,
+    stable_sort_by_key_copy_batch,
 )
 
 __version__ = "1.0.0"

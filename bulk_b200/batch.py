@@ -50,6 +50,14 @@ def sort_item_type(key: str, value: str):
                 {"_fields_": [("keys", ctypes.c_void_p), ("vals", ctypes.c_void_p), ("n", ctypes.c_uint64)]})
 
 
+@lru_cache(maxsize=None)
+def sort_copy_item_type(key: str, value: str):
+    """ctypes mirror of bk_sort_copy_item_<key>_<value>."""
+    return type(f"bk_sort_copy_item_{key}_{value}", (ctypes.Structure,),
+                {"_fields_": [("in_keys", ctypes.c_void_p), ("in_vals", ctypes.c_void_p), ("keys", ctypes.c_void_p),
+                              ("vals", ctypes.c_void_p), ("n", ctypes.c_uint64)]})
+
+
 def batch_workspace_bytes(algo: str, key: str, value: str | None, sizes) -> int:
     arr = (ctypes.c_uint64 * max(len(sizes), 1))(*sizes)
     return lib.bk_batch_workspace_bytes(_lib.ALGO[algo], _lib.DTYPE[key], _lib.DTYPE[value], arr, len(sizes))
@@ -179,3 +187,44 @@ def stable_sort_by_key_batch(keys_list, vals_list, stream: torch.cuda.Stream | N
             ws, wsb = workspaces.get(max(need, 256), dev, so)
             check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
     return keys_list, vals_list
+
+
+def stable_sort_by_key_copy_batch(in_keys, in_vals, out_keys=None, out_vals=None,
+                                  stream: torch.cuda.Stream | None = None):
+    """Stable sort of every (in_keys[i], in_vals[i]) pair into (out_keys[i],
+    out_vals[i]) (allocated when not given); the inputs are left unchanged.
+    Returns (out_keys, out_vals)."""
+    in_keys, in_vals = list(in_keys), list(in_vals)
+    if len(in_keys) != len(in_vals):
+        raise ValueError("in_keys and in_vals must have the same length")
+    out_keys = list(out_keys) if out_keys is not None else [torch.empty_like(k) for k in in_keys]
+    out_vals = list(out_vals) if out_vals is not None else [torch.empty_like(v) for v in in_vals]
+    if not in_keys:
+        return out_keys, out_vals
+    dev = _require_cuda(*in_keys, *in_vals, *out_keys, *out_vals)
+    kt = dtype_tag(in_keys[0].dtype)
+    vsize = in_vals[0].element_size()
+    if vsize not in (4, 8):
+        raise TypeError("payloads must be 4 or 8 bytes")
+    vt = "u32" if vsize == 4 else "u64"
+    for k, v, ok, ov in zip(in_keys, in_vals, out_keys, out_vals):
+        if dtype_tag(k.dtype) != kt or v.element_size() != vsize or ok.dtype != k.dtype or \
+                ov.element_size() != vsize:
+            raise TypeError("one key dtype and one payload size per batch")
+        if not (k.numel() == v.numel() == ok.numel() == ov.numel()):
+            raise ValueError("every array of an item must have the same length")
+    so = _stream_obj(stream, dev)
+    s = so.cuda_stream
+    item_t = sort_copy_item_type(kt, vt)
+    fn = getattr(lib, f"bk_sort_by_key_{kt}_{vt}_copy_batch")
+    for lo, hi in _chunks(len(in_keys)):
+        items = (item_t * (hi - lo))()
+        for j, i in enumerate(range(lo, hi)):
+            it = items[j]
+            it.in_keys, it.in_vals = in_keys[i].data_ptr(), in_vals[i].data_ptr()
+            it.keys, it.vals, it.n = out_keys[i].data_ptr(), out_vals[i].data_ptr(), in_keys[i].numel()
+        need = batch_workspace_bytes("sort_by_key", kt, vt, [in_keys[i].numel() for i in range(lo, hi)])
+        with torch.cuda.device(dev):
+            ws, wsb = workspaces.get(max(need, 256), dev, so)
+            check(fn(ctypes.cast(items, ctypes.c_void_p), hi - lo, ws, wsb, s), fn.__name__)
+    return out_keys, out_vals

@@ -119,6 +119,8 @@ struct RsTile {
   P *vals;
   K *tk;
   P *tv;
+  const K *src_k;       // what the first pass reads (keys, or a separate source)
+  const P *src_v;
   uint64_t n;
   uint32_t local;
   uint32_t tiles;       // the array's tiles
@@ -135,7 +137,7 @@ struct RsOne {
   uint64_t n;
   uint32_t tiles;
   __device__ __forceinline__ RsTile<K, P> tile(unsigned int g) const {
-    return RsTile<K, P>{keys, vals, tk, tv, n, g, tiles, 0ull, 0u};
+    return RsTile<K, P>{keys, vals, tk, tv, keys, vals, n, g, tiles, 0ull, 0u};
   }
 };
 
@@ -144,6 +146,8 @@ template <typename K, typename P>
 struct RsBatch {
   K *keys[kRsBatchMax];
   P *vals[kRsBatchMax];
+  const K *src_k[kRsBatchMax];  // what the first pass reads
+  const P *src_v[kRsBatchMax];
   K *tk[kRsBatchMax];
   P *tv[kRsBatchMax];
   uint64_t n[kRsBatchMax];
@@ -157,7 +161,8 @@ struct RsBatch {
       if (start[mid] <= g) lo = mid;
       else hi = mid - 1;
     }
-    return RsTile<K, P>{keys[lo], vals[lo], tk[lo], tv[lo], n[lo], g - start[lo], start[lo + 1] - start[lo],
+    return RsTile<K, P>{keys[lo], vals[lo], tk[lo], tv[lo], src_k[lo], src_v[lo], n[lo], g - start[lo],
+                        start[lo + 1] - start[lo],
                         (uint64_t)start[lo] * kRsBins, elem_base[lo]};
   }
 };
@@ -174,9 +179,9 @@ __device__ __forceinline__ void rs_prefetch_tile(const Src &src, unsigned int g,
   const RsTile<K, P> f = src.tile(g);
   const uint64_t base = (uint64_t)f.local * kRsTile;
   const uint64_t cnt = (f.n - base) < (uint64_t)kRsTile ? (f.n - base) : (uint64_t)kRsTile;
-  prefetch_l2_range(((pass & 1) ? f.tk : f.keys) + base, cnt * sizeof(K));
+  prefetch_l2_range(((pass & 1) ? f.tk : (pass == 0 ? f.src_k : f.keys)) + base, cnt * sizeof(K));
   if constexpr (has_payload<P>()) {
-    if (payload) prefetch_l2_range(((pass & 1) ? f.tv : f.vals) + base, cnt * sizeof(P));
+    if (payload) prefetch_l2_range(((pass & 1) ? f.tv : (pass == 0 ? f.src_v : f.vals)) + base, cnt * sizeof(P));
   }
 }
 
@@ -188,7 +193,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_upsweep_kernel(const __grid_con
   const int shift = 8 * pass;
   if (tid == 0 && ahead != 0) rs_prefetch_tile<K, P>(src, blockIdx.x + ahead, pass, false);
   const RsTile<K, P> tl = src.tile(blockIdx.x);
-  const K *in_k = (pass & 1) ? tl.tk : tl.keys;
+  const K *in_k = (pass & 1) ? tl.tk : (pass == 0 ? tl.src_k : tl.keys);
   const uint64_t tbase = (uint64_t)tl.local * kRsTile;
   const int count = (int)((tl.n - tbase) < (uint64_t)kRsTile ? (tl.n - tbase) : (uint64_t)kRsTile);
 #pragma unroll
@@ -248,8 +253,8 @@ __global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downswe
   const int shift = 8 * pass;
   if (tid == 0 && ahead != 0) rs_prefetch_tile<K, P>(src, blockIdx.x + ahead, pass, true);
   const RsTile<K, P> tl = src.tile(blockIdx.x);
-  const K *in_k = (pass & 1) ? tl.tk : tl.keys;
-  const P *in_v = (pass & 1) ? tl.tv : tl.vals;
+  const K *in_k = (pass & 1) ? tl.tk : (pass == 0 ? tl.src_k : tl.keys);
+  const P *in_v = (pass & 1) ? tl.tv : (pass == 0 ? tl.src_v : tl.vals);
   K *out_k = (pass & 1) ? tl.keys : tl.tk;
   P *out_v = (pass & 1) ? tl.vals : tl.tv;
   const uint64_t tbase = (uint64_t)tl.local * kRsTile;
@@ -459,9 +464,12 @@ int radix_sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes,
   return radix_sort_run<K, P>(RsOne<K, P>{keys, vals, tk, tv, n, (uint32_t)L.tiles}, L, ws, stream);
 }
 
-// A batch item as the C-ABI passes it.
+// A batch item: sort in_keys / in_vals (left unchanged) into keys / vals;
+// in place when they are the same arrays.
 template <typename K, typename P>
 struct RsItem {
+  const K *in_keys;
+  const P *in_vals;
   K *keys;
   P *vals;
   uint64_t n;
@@ -479,10 +487,22 @@ int radix_sort_batch_launch(const RsItem<K, P> *items, uint32_t count, void *d_w
   uint32_t m = 0;
   for (uint32_t i = 0; i < count; ++i) {
     const RsItem<K, P> &it = items[i];
-    if (it.n > 0 && (it.keys == nullptr || (has_payload<P>() && it.vals == nullptr))) return BK_ERR_INVALID_ARGUMENT;
-    if (!host::aligned_to<K>(it.keys)) return BK_ERR_MISALIGNED;
+    if (it.n > 0 && (it.keys == nullptr || it.in_keys == nullptr ||
+                     (has_payload<P>() && (it.vals == nullptr || it.in_vals == nullptr))))
+      return BK_ERR_INVALID_ARGUMENT;
+    if (!host::aligned_to<K>(it.keys) || !host::aligned_to<K>(it.in_keys)) return BK_ERR_MISALIGNED;
     if constexpr (has_payload<P>()) {
-      if (!host::aligned_to<P>(it.vals)) return BK_ERR_MISALIGNED;
+      if (!host::aligned_to<P>(it.vals) || !host::aligned_to<P>(it.in_vals)) return BK_ERR_MISALIGNED;
+    }
+    if (it.n == 1 && it.in_keys != it.keys) {  // a single element out of place: copied, not sorted
+      if ((st = host::from_cuda(cudaMemcpyAsync(it.keys, it.in_keys, sizeof(K), cudaMemcpyDeviceToDevice,
+                                                stream))) != BK_OK)
+        return st;
+      if constexpr (has_payload<P>()) {
+        if ((st = host::from_cuda(cudaMemcpyAsync(it.vals, it.in_vals, sizeof(P), cudaMemcpyDeviceToDevice,
+                                                  stream))) != BK_OK)
+          return st;
+      }
     }
     if (it.n >= kRsMaxN) return BK_ERR_TOO_LARGE;
     if (it.n > 1) sz[m++] = it.n;
@@ -502,6 +522,8 @@ int radix_sort_batch_launch(const RsItem<K, P> *items, uint32_t count, void *d_w
     const uint32_t k = b.count++;
     b.keys[k] = it.keys;
     b.vals[k] = it.vals;
+    b.src_k[k] = it.in_keys;
+    b.src_v[k] = it.in_vals;
     b.tk[k] = reinterpret_cast<K *>(ws + off);
     off += align_up(it.n * sizeof(K), 256);
     b.tv[k] = reinterpret_cast<P *>(ws + off);

@@ -10,9 +10,10 @@
 // streams of their own (forked from the caller's stream and joined back to
 // it, each with its own slice of the workspace) so that a round's sorts,
 // reduce_by_keys and scans run side by side on the device; a kind with a
-// single request in the round is issued as a plain single-array call.  Its
-// one kernel gathers the sort requests' input windows into their own
-// buffers for a whole batch in a single launch.
+// single request in the round is issued as a plain single-array call, and a
+// round of at most two requests as plain calls on the caller's stream.  A
+// round's sorts run out of place: the batched sort reads each request's
+// source window and writes the request's own buffers.
 #include <algorithm>
 #include <chrono>
 #include <deque>
@@ -84,39 +85,6 @@ class Pool {
   std::unordered_map<uint64_t, uint64_t> used_;
   uint64_t in_use_ = 0, high_ = 0;
 };
-
-// ---------------------------------------------------------------------------
-// Gather copy: copy i moves words[i] 4-byte words from src[i] to dst[i]; all
-// pointers are 16-byte aligned.  Thread u of the grid-stride loop owns the
-// 16-byte unit u of the concatenation (units[i] is the first unit of copy i)
-// and copies only the words of its unit that belong to the copy.
-constexpr int kGatherMax = 256;
-struct GatherBatch {
-  const uint32_t *src[kGatherMax];
-  uint32_t *dst[kGatherMax];
-  uint64_t words[kGatherMax];
-  uint64_t units[kGatherMax + 1];
-  uint32_t count;
-};
-
-__global__ void __launch_bounds__(256) gather_kernel(const __grid_constant__ GatherBatch b) {
-  const uint64_t total = b.units[b.count];
-  for (uint64_t u = blockIdx.x * 256ull + threadIdx.x; u < total; u += (uint64_t)gridDim.x * 256ull) {
-    int lo = 0, hi = (int)b.count - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (b.units[mid] <= u) lo = mid;
-      else hi = mid - 1;
-    }
-    const uint64_t w = (u - b.units[lo]) * 4;
-    const uint64_t left = b.words[lo] - w;
-    if (left >= 4) {
-      *reinterpret_cast<uint4 *>(b.dst[lo] + w) = *reinterpret_cast<const uint4 *>(b.src[lo] + w);
-    } else {
-      for (uint64_t k = 0; k < left; ++k) b.dst[lo][w + k] = b.src[lo][w + k];
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 struct Req {
@@ -330,14 +298,27 @@ class Loop {
     }
   }
 
+  static constexpr int kPlainRound = 2;
+
   // One admission round: per kind, one batched call (at most BK_BATCH_MAX
-  // arrays each; the sort inputs gathered first, 128 requests per gather
-  // launch), or a plain call for a kind with one request.  With more than
+  // arrays each; sorts out of place, from the requests' source windows), or
+  // a plain call for a kind with one request.  With more than
   // one kind present, each kind runs on its own stream, forked from the
   // caller's stream and joined back to it; otherwise the kind runs on the
   // caller's stream (its slice is free there: the caller's stream has
   // joined every earlier use of it).
   int issue_batches(const std::vector<Req *> &reqs) {
+    // a round of one or two requests (light load) is issued as plain calls on
+    // the caller's stream: batch descriptors and stream fork/join would only
+    // add latency there
+    if (reqs.size() <= (size_t)kPlainRound) {
+      for (Req *r : reqs) {
+        const int kind = (int)r->r->kind;
+        const int st = issue_one_on(r, st_, ws_[kind], ws_bytes_[kind]);
+        if (st != BK_OK) return st;
+      }
+      return BK_OK;
+    }
     std::vector<Req *> by[3];
     for (Req *r : reqs) by[r->r->kind].push_back(r);
     const int kinds = (by[0].empty() ? 0 : 1) + (by[1].empty() ? 0 : 1) + (by[2].empty() ? 0 : 1);
@@ -365,41 +346,23 @@ class Loop {
 
   // One kind's batched calls on stream s with the kind's workspace slice.
   int issue_kind(int kind, const std::vector<Req *> &v, cudaStream_t s) {
-    int st;
+    int st = BK_OK;
     void *ws = ws_[kind];
     const size_t wsb = ws_bytes_[kind];
-    for (size_t lo = 0; kind == BK_SERVE_SORT && lo < v.size(); lo += kGatherMax / 2) {
-      const size_t hi = std::min(v.size(), lo + kGatherMax / 2);
-      GatherBatch g;
-      g.count = 0;
-      g.units[0] = 0;
-      for (size_t i = lo; i < hi; ++i) {
-        const Req *q = v[i];
-        const uint64_t n = q->r->n, o = q->r->src_offset;
-        const uint32_t *srcs[2] = {c_.sort_keys + o, c_.sort_vals + o};
-        for (int b = 0; b < 2; ++b) {
-          const uint32_t c = g.count++;
-          g.src[c] = srcs[b];
-          g.dst[c] = buf<uint32_t>(q, b);
-          g.words[c] = n;
-          g.units[c + 1] = g.units[c] + (n + 3) / 4;
-        }
-      }
-      const uint64_t units = g.units[g.count];
-      if (units == 0) continue;
-      const unsigned grid = (unsigned)std::min<uint64_t>((units + 255) / 256, 148ull * 8);
-      gather_kernel<<<grid, 256, 0, s>>>(g);
-      if ((st = host::launch_status()) != BK_OK) return st;
-    }
     for (size_t lo = 0; lo < v.size(); lo += BK_BATCH_MAX) {
       const size_t hi = std::min(v.size(), lo + (size_t)BK_BATCH_MAX);
       ++calls_;
       ++batches_;
       if (kind == BK_SERVE_SORT) {
-        bk_sort_item_u32_u32 it[BK_BATCH_MAX];
-        for (size_t i = lo; i < hi; ++i)
-          it[i - lo] = bk_sort_item_u32_u32{buf<uint32_t>(v[i], 0), buf<uint32_t>(v[i], 1), v[i]->r->n};
-        st = bk_sort_by_key_u32_u32_batch(it, (uint32_t)(hi - lo), ws, wsb, (bk_stream_t)s);
+        // out of place: the first radix pass reads each request's source
+        // window and the result lands in its own buffers (no separate copy)
+        bk_sort_copy_item_u32_u32 it[BK_BATCH_MAX];
+        for (size_t i = lo; i < hi; ++i) {
+          const uint64_t o = v[i]->r->src_offset;
+          it[i - lo] = bk_sort_copy_item_u32_u32{c_.sort_keys + o, c_.sort_vals + o, buf<uint32_t>(v[i], 0),
+                                                 buf<uint32_t>(v[i], 1), v[i]->r->n};
+        }
+        st = bk_sort_by_key_u32_u32_copy_batch(it, (uint32_t)(hi - lo), ws, wsb, (bk_stream_t)s);
       } else if (kind == BK_SERVE_RBK) {
         bk_rbk_item_i32_f32 it[BK_BATCH_MAX];
         for (size_t i = lo; i < hi; ++i) {

@@ -25,7 +25,9 @@ int radix_sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes,
 template <typename K, typename P>
 size_t radix_sort_ws_bytes(uint64_t n);
 template <typename K, typename P>
-struct RsItem {
+struct RsItem {  // as radix_sort.cu defines it: in_* sorted into keys / vals
+  const K *in_keys;
+  const P *in_vals;
   K *keys;
   P *vals;
   uint64_t n;
@@ -431,6 +433,15 @@ struct SortItem {
   P *vals;
   uint64_t n;
 };
+// Out of place: in_keys / in_vals (left unchanged) sorted into keys / vals.
+template <typename K, typename P>
+struct SortCopyItem {
+  const K *in_keys;
+  const P *in_vals;
+  K *keys;
+  P *vals;
+  uint64_t n;
+};
 
 // Workspace of a batch: per array (n > 1), its key and payload temporaries
 // and its merge-pass splits, one after another.
@@ -467,14 +478,29 @@ size_t sort_batch_ws_bytes_t(const uint64_t *sizes, uint32_t count) {
 }
 
 template <typename K, typename P>
+int sort_batch_copy_launch(const SortCopyItem<K, P> *items, uint32_t count, void *d_ws, size_t ws_bytes,
+                           cudaStream_t stream);
+
+// In place: the copy form with each array as its own source.
+template <typename K, typename P>
 int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
+  if (count > 0 && items == nullptr) return BK_ERR_INVALID_ARGUMENT;
+  if (count > (uint32_t)kSortBatchMax) return BK_ERR_TOO_LARGE;
+  SortCopyItem<K, P> c[kSortBatchMax];
+  for (uint32_t i = 0; i < count; ++i) c[i] = SortCopyItem<K, P>{items[i].keys, items[i].vals, items[i].keys, items[i].vals, items[i].n};
+  return sort_batch_copy_launch<K, P>(c, count, d_ws, ws_bytes, stream);
+}
+
+template <typename K, typename P>
+int sort_batch_copy_launch(const SortCopyItem<K, P> *items, uint32_t count, void *d_ws, size_t ws_bytes,
+                           cudaStream_t stream) {
   using C = SortCfg<K>;
   if (count > 0 && items == nullptr) return BK_ERR_INVALID_ARGUMENT;
   if (count > (uint32_t)kSortBatchMax) return BK_ERR_TOO_LARGE;
   {
     uint64_t sizes[kSortBatchMax];
     for (uint32_t i = 0; i < count; ++i) sizes[i] = items[i].n;
-    static_assert(sizeof(SortItem<K, P>) == sizeof(RsItem<K, P>), "same item layout");
+    static_assert(sizeof(SortCopyItem<K, P>) == sizeof(RsItem<K, P>), "same item layout");
     if (sort_batch_radix<K, P>(sizes, count))
       return radix_sort_batch_launch<K, P>(reinterpret_cast<const RsItem<K, P> *>(items), count, d_ws, ws_bytes,
                                            stream);
@@ -497,6 +523,9 @@ int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, s
   uint64_t sizes[kSortBatchMax];
   for (uint32_t i = 0; i < count; ++i) {
     if ((st = sort_check_array(items[i].keys, items[i].vals, items[i].n)) != BK_OK) return st;
+    if ((st = sort_check_array(const_cast<K *>(items[i].in_keys), const_cast<P *>(items[i].in_vals), items[i].n)) !=
+        BK_OK)
+      return st;
     sizes[i] = items[i].n;
   }
   st = host::check_ws(d_ws, ws_bytes, merge_sort_batch_ws_bytes_t<K, P>(sizes, count));
@@ -508,6 +537,16 @@ int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, s
   bs.count = 0;
   for (uint32_t i = 0; i < count; ++i) {
     const uint64_t n = items[i].n;
+    if (n == 1 && items[i].in_keys != items[i].keys) {  // a single element out of place: copied
+      if ((st = host::from_cuda(cudaMemcpyAsync(items[i].keys, items[i].in_keys, sizeof(K), cudaMemcpyDeviceToDevice,
+                                                stream))) != BK_OK)
+        return st;
+      if constexpr (has_payload<P>()) {
+        if ((st = host::from_cuda(cudaMemcpyAsync(items[i].vals, items[i].in_vals, sizeof(P),
+                                                  cudaMemcpyDeviceToDevice, stream))) != BK_OK)
+          return st;
+      }
+    }
     if (n <= 1) continue;  // already sorted
     Arr &a = arr[na++];
     a.keys = items[i].keys;
@@ -523,8 +562,8 @@ int sort_batch_launch(const SortItem<K, P> *items, uint32_t count, void *d_ws, s
     max_passes = a.passes > max_passes ? a.passes : max_passes;
     // an odd number of passes starts in the temporaries so the last lands in place
     const uint32_t k = bs.count++;
-    bs.in_k[k] = a.keys;
-    bs.in_v[k] = a.vals;
+    bs.in_k[k] = items[i].in_keys;  // the block sort reads the source (the array itself in place)
+    bs.in_v[k] = items[i].in_vals;
     bs.out_k[k] = (a.passes & 1) ? a.tk : a.keys;
     bs.out_v[k] = (a.passes & 1) ? a.tv : a.vals;
     bs.n[k] = n;
@@ -626,9 +665,19 @@ BK_DEFINE_SORT(f64, double)
     return bk::sort_batch_launch<K, VI>(reinterpret_cast<const bk::SortItem<K, VI> *>(items), count, d_ws,    \
                                         ws_bytes, (cudaStream_t)stream);                                      \
   }
+#define BK_DEFINE_SORT_COPY_BATCH(KN, K, VN, V, VI)                                                             \
+  static_assert(sizeof(bk_sort_copy_item_##KN##_##VN) == sizeof(bk::SortCopyItem<K, VI>), "bk_sort_copy_item");  \
+  extern "C" int bk_sort_by_key_##KN##_##VN##_copy_batch(const bk_sort_copy_item_##KN##_##VN *items,          \
+                                                         uint32_t count, void *d_ws, size_t ws_bytes,          \
+                                                         bk_stream_t stream) {                                 \
+    return bk::sort_batch_copy_launch<K, VI>(reinterpret_cast<const bk::SortCopyItem<K, VI> *>(items), count,   \
+                                             d_ws, ws_bytes, (cudaStream_t)stream);                             \
+  }
 #define BK_DEFINE_SORT_BATCH_K(KN, K)                                 \
   BK_DEFINE_SORT_BATCH(KN, K, u32, uint32_t, uint32_t)                \
-  BK_DEFINE_SORT_BATCH(KN, K, u64, uint64_t, unsigned long long)
+  BK_DEFINE_SORT_BATCH(KN, K, u64, uint64_t, unsigned long long)      \
+  BK_DEFINE_SORT_COPY_BATCH(KN, K, u32, uint32_t, uint32_t)           \
+  BK_DEFINE_SORT_COPY_BATCH(KN, K, u64, uint64_t, unsigned long long)
 
 BK_DEFINE_SORT_BATCH_K(i32, int32_t)
 BK_DEFINE_SORT_BATCH_K(u32, uint32_t)

@@ -329,6 +329,36 @@ BK_API int bk_sort_by_key_f32_u32_batch(const bk_sort_item_f32_u32 *items, uint3
 BK_API int bk_sort_by_key_f32_u64_batch(const bk_sort_item_f32_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_sort_by_key_f64_u32_batch(const bk_sort_item_f64_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_sort_by_key_f64_u64_batch(const bk_sort_item_f64_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+/* Out-of-place form of the batched sort: for each item, in_keys / in_vals
+ * (left unchanged) are stably sorted into keys / vals (n elements each; the
+ * ranges must not overlap).  The first pass reads the sources directly, so a
+ * caller that would copy each input window before an in-place sort saves
+ * that copy.  Workspace as for the in-place batch.  No counterpart in the
+ * reference (its sort is in place, merge_sort_by_key.cu:150-209). */
+typedef struct bk_sort_copy_item_i32_u32 { const int32_t *in_keys; const uint32_t *in_vals; int32_t *keys; uint32_t *vals; uint64_t n; } bk_sort_copy_item_i32_u32;
+typedef struct bk_sort_copy_item_i32_u64 { const int32_t *in_keys; const uint64_t *in_vals; int32_t *keys; uint64_t *vals; uint64_t n; } bk_sort_copy_item_i32_u64;
+typedef struct bk_sort_copy_item_u32_u32 { const uint32_t *in_keys; const uint32_t *in_vals; uint32_t *keys; uint32_t *vals; uint64_t n; } bk_sort_copy_item_u32_u32;
+typedef struct bk_sort_copy_item_u32_u64 { const uint32_t *in_keys; const uint64_t *in_vals; uint32_t *keys; uint64_t *vals; uint64_t n; } bk_sort_copy_item_u32_u64;
+typedef struct bk_sort_copy_item_i64_u32 { const int64_t *in_keys; const uint32_t *in_vals; int64_t *keys; uint32_t *vals; uint64_t n; } bk_sort_copy_item_i64_u32;
+typedef struct bk_sort_copy_item_i64_u64 { const int64_t *in_keys; const uint64_t *in_vals; int64_t *keys; uint64_t *vals; uint64_t n; } bk_sort_copy_item_i64_u64;
+typedef struct bk_sort_copy_item_u64_u32 { const uint64_t *in_keys; const uint32_t *in_vals; uint64_t *keys; uint32_t *vals; uint64_t n; } bk_sort_copy_item_u64_u32;
+typedef struct bk_sort_copy_item_u64_u64 { const uint64_t *in_keys; const uint64_t *in_vals; uint64_t *keys; uint64_t *vals; uint64_t n; } bk_sort_copy_item_u64_u64;
+typedef struct bk_sort_copy_item_f32_u32 { const float *in_keys; const uint32_t *in_vals; float *keys; uint32_t *vals; uint64_t n; } bk_sort_copy_item_f32_u32;
+typedef struct bk_sort_copy_item_f32_u64 { const float *in_keys; const uint64_t *in_vals; float *keys; uint64_t *vals; uint64_t n; } bk_sort_copy_item_f32_u64;
+typedef struct bk_sort_copy_item_f64_u32 { const double *in_keys; const uint32_t *in_vals; double *keys; uint32_t *vals; uint64_t n; } bk_sort_copy_item_f64_u32;
+typedef struct bk_sort_copy_item_f64_u64 { const double *in_keys; const uint64_t *in_vals; double *keys; uint64_t *vals; uint64_t n; } bk_sort_copy_item_f64_u64;
+BK_API int bk_sort_by_key_i32_u32_copy_batch(const bk_sort_copy_item_i32_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i32_u64_copy_batch(const bk_sort_copy_item_i32_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u32_u32_copy_batch(const bk_sort_copy_item_u32_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u32_u64_copy_batch(const bk_sort_copy_item_u32_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i64_u32_copy_batch(const bk_sort_copy_item_i64_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_i64_u64_copy_batch(const bk_sort_copy_item_i64_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u64_u32_copy_batch(const bk_sort_copy_item_u64_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_u64_u64_copy_batch(const bk_sort_copy_item_u64_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f32_u32_copy_batch(const bk_sort_copy_item_f32_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f32_u64_copy_batch(const bk_sort_copy_item_f32_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f64_u32_copy_batch(const bk_sort_copy_item_f64_u32 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_sort_by_key_f64_u64_copy_batch(const bk_sort_copy_item_f64_u64 *items, uint32_t count, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
 /* ---- serving loop -----------------------------------------------------------
  * No counterpart in the reference, whose drivers run one array at a time.

@@ -216,3 +216,29 @@ def test_sort_batch_matches_each_array_alone(cuda, kv):
         order = np.argsort(k, kind="stable")
         assert np.array_equal(host(gk), k[order]), f"n={k.size}"
         assert np.array_equal(host(gv), v[order]), f"n={k.size}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kv", [("u32", "u32"), ("f32", "u32"), ("u64", "u64")])
+@pytest.mark.parametrize("sizes", [[0, 1, 2, 100, 4095, 8193, 20000, 300001, 7],   # radix passes
+                                   [0, 1, 5, 300, 4096, 17]])                     # one block sort
+def test_sort_copy_batch_reads_the_sources_and_leaves_them(cuda, kv, sizes):
+    """Out of place: each (in_keys, in_vals) sorted stably into its own
+    outputs, the sources unchanged (the first radix pass, or the block sort,
+    reads them directly)."""
+    from tests.gpu_util import NP, dev, host
+    kt, vt = kv
+    keys_h, vals_h = [], []
+    for i, n in enumerate(sizes):
+        rng = np.random.default_rng(700 + i)
+        k = (rng.integers(0, 50, n) / 4).astype(NP[kt]) if kt == "f32" else \
+            rng.integers(0, 1000 if i % 2 else 1 << 30, n).astype(NP[kt])
+        keys_h.append(k)
+        vals_h.append(np.arange(n, dtype=NP[vt]))
+    dk = [dev(k) for k in keys_h]
+    dv = [dev(v) for v in vals_h]
+    ok, ov = bulk_b200.stable_sort_by_key_copy_batch(dk, dv)
+    for k, v, gk, gv, sk, sv in zip(keys_h, vals_h, ok, ov, dk, dv):
+        order = np.argsort(k, kind="stable")
+        assert np.array_equal(host(gk), k[order]) and np.array_equal(host(gv), v[order]), f"n={k.size}"
+        assert np.array_equal(host(sk), k) and np.array_equal(host(sv), v), f"source changed, n={k.size}"
