@@ -525,6 +525,14 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
       armpar ^= 1u << bn;
       armany |= 1u << bn;
       next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
+      // tiles are ticketed about in order, gridDim.x per iteration: ask L2 now
+      // for the one some CTA will load 1 iteration(s) from now
+      if (tn != NONE && tn + 1u * gridDim.x < num_tiles) {
+        const RbkTile<K, V> f = src.tile(tn + 1u * gridDim.x);
+        const uint64_t fb = (uint64_t)f.local * TILE;
+        prefetch_l2_range(f.keys + fb, (uint64_t)f.count() * sizeof(K));
+        prefetch_l2_range(f.vals + fb, (uint64_t)f.count() * sizeof(V));
+      }
       // re-read t_{i-1} into t's buffer once phase 1 of t is done with it
       if (!mbar_wait_or_abort(&s_p1[bt], (p1par >> bt) & 1u, spin_limit_ns, &s_abort)) {
         record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
