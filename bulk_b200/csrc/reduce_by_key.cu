@@ -630,6 +630,11 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
     unsigned int t = NONE;
     if (!mbar_wait_or_abort(&s_full[bt], (fpar >> bt) & 1u, spin_limit_ns, &s_abort)) bad = true;
     fpar ^= 1u << bt;
+    // the marks this thread stored last iteration are read back by a TMA copy
+    // that the loader issues once this iteration's phase 1 is done: order them
+    // before it now, an iteration after the stores (fencing right after them
+    // would wait for their round trip to L2)
+    fence_proxy_async_global();
     bad = __any_sync(0xffffffffu, bad);
     if (!bad) t = s_ticket[bt];
     // tiles without a TMA copy: the compute warps stage them here, between
@@ -664,7 +669,6 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
         *reinterpret_cast<uint4 *>(ms + (SWZ ? lo.v[c] : e0 * (uint32_t)sizeof(V) + 16u * c)) = q;
       }
       const P incl = warp_inclusive_scan(lane_agg, op, lane);
-      fence_proxy_async_global();  // the marks are read back by a TMA copy
       if (lane == 31) s_wagg[it & 3][warp] = incl;
       P lex = shfl_up(incl, 1);
       if (lane == 0) lex = OpSeg<V>::identity();
