@@ -15,12 +15,17 @@
 // the sum of the values since the last head.  (c1,v1) (+) (c2,v2) =
 // (c1 + c2, c2 ? v2 : v1 + v2) is associative but not commutative, so every
 // fold keeps data order.  At each tail (last element of a run) the inclusive
-// (c, v) gives the run's output slot c - 1 and its sum v.  The tile pipeline
-// is the scan's (scan.cu): persistent CTAs whose compute warps, loader lane
-// and look-back warp hand over through mbarriers; three tile buffers rotate
-// through prefetch (keys, values and a one-key halo on each side, by TMA),
-// phase 1 (the tile aggregate, published), a re-read from L2 and phase 2
-// (the tile's runs, emitted once the look-back warp has found the prefix).
+// (c, v) gives the run's output slot c - 1 and its sum v.  Persistent CTAs
+// take tiles from an atomic ticket; a loader lane brings each tile (keys,
+// values and a one-key halo on each side) into shared memory by TMA, the
+// compute warps reduce it (phase 1: the tile aggregate, published at once),
+// compact the runs that end in it -- key and tile-local sum, in output order
+// -- and copy them to a run slot of the CTA's ring in global memory, which
+// frees the tile buffer for the next load; a look-back warp finds the tile's
+// exclusive prefix meanwhile.  Two iterations later the compute warps copy the
+// runs from the ring (L2) to the output at the prefix's run count, adding the
+// prefix's sum to a run that began in an earlier tile (phase 2).  No element
+// is read twice: only the runs wait for the prefix.
 #include <algorithm>
 
 #include "bk_common.cuh"
@@ -49,7 +54,6 @@ struct OpSeg {
 
 constexpr int kRbkWarps = 8;                       // compute warps (0-7)
 constexpr int kRbkThreads = 32 * (kRbkWarps + 2);  // + the loader warp (8; one lane works) + the look-back warp (9)
-constexpr int kRbkBufs = 3;                        // tile buffers in rotation (as in scan.cu)
 constexpr int kRbkQueue = 4;                       // look-back queue entries
 
 template <typename K, typename V>
@@ -64,6 +68,12 @@ struct RbkCfg {
   static constexpr size_t KEY_BYTES = align_up(sizeof(K) * TILE, 1024);
   static constexpr size_t VAL_BYTES = align_up(sizeof(V) * TILE, 1024);
   static constexpr size_t BUF_BYTES = KEY_BYTES + VAL_BYTES;
+  // tile buffers in rotation: a tile holds one from its load, D iterations
+  // before its phase 1, to the end of its phase 1, so NB = D + 1; two CTAs per
+  // SM keep NB * BUF_BYTES under half the SM's shared memory
+  static constexpr int NB = BUF_BYTES <= 24 * 1024 ? 4 : 3;
+  static constexpr int D = NB - 1;
+  static constexpr size_t RUN_SLOT_BYTES = (sizeof(K) + sizeof(V)) * TILE;  // a tile's runs, at most TILE
   static constexpr int KCH = M * (int)sizeof(K) / 16;  // 16-byte chunks of a lane's keys
   static constexpr int VCH = M * (int)sizeof(V) / 16;  // ... and of its values
   using P = Seg<V>;
@@ -74,9 +84,10 @@ template <typename K, typename V>
 size_t rbk_num_tiles(uint64_t n) {
   return (size_t)((n + RbkCfg<K, V>::TILE - 1) / RbkCfg<K, V>::TILE);
 }
-// Workspace: the header, one look-back status per tile, then the tail-mark
-// ring: three tile-sized value slots per persistent CTA (phase 1 of a tile
-// writes its running values there; the re-read for phase 2 brings them back).
+// Workspace: the header, one look-back status per tile, then the run ring:
+// kRbkRunSlots run slots per persistent CTA (a tile's runs wait there, keys
+// then values, from its phase 1 to its phase 2).
+constexpr int kRbkRunSlots = 4;
 constexpr size_t kRbkMaxGrid = 320;  // persistent CTAs at most (2 per SM)
 template <typename K, typename V>
 size_t rbk_ring_offset(size_t tiles) {
@@ -84,8 +95,8 @@ size_t rbk_ring_offset(size_t tiles) {
 }
 template <typename K, typename V>
 size_t rbk_ws_for_tiles(size_t tiles) {
-  const size_t slots = 3 * (tiles < kRbkMaxGrid ? tiles : kRbkMaxGrid);
-  return rbk_ring_offset<K, V>(tiles) + slots * RbkCfg<K, V>::TILE * sizeof(V);
+  const size_t ctas = tiles < kRbkMaxGrid ? tiles : kRbkMaxGrid;
+  return rbk_ring_offset<K, V>(tiles) + ctas * kRbkRunSlots * RbkCfg<K, V>::RUN_SLOT_BYTES;
 }
 template <typename K, typename V>
 size_t rbk_ws_bytes(uint64_t n) {
@@ -115,7 +126,7 @@ struct RbkTile {
   K *out_keys;
   V *out_vals;
   uint64_t *num_out;
-  bool tma;        // the loader brings this tile (and its re-read) in by TMA
+  bool tma;        // the loader brings this tile in by TMA
   __device__ __forceinline__ uint32_t count() const {
     const uint64_t base = (uint64_t)local * RbkCfg<K, V>::TILE;
     return (uint32_t)((n - base) < (uint64_t)RbkCfg<K, V>::TILE ? (n - base) : (uint64_t)RbkCfg<K, V>::TILE);
@@ -186,8 +197,7 @@ struct RbkBatch {
   __device__ __forceinline__ const CUtensorMap *val_map() const { return nullptr; }
 };
 
-// Byte offset of byte o of a tile area in shared memory (and in a mark-ring
-// slot, which holds an image of the values area): swizzled for tiles that
+// Byte offset of byte o of a tile area in shared memory: swizzled for tiles that
 // arrive by tensor copies, linear otherwise.
 template <bool SWZ>
 __device__ __forceinline__ uint32_t area_off(uint32_t o) {
@@ -239,35 +249,6 @@ __device__ __forceinline__ bool rbk_issue_load(const Src &src, const RbkTile<K, 
   return true;
 }
 
-// Loader: re-read tile `tl` for phase 2 into buffer `buf`: its keys from the
-// input (L2) and, in place of its values, the running values phase 1 left in
-// the mark slot `slot` (an image of the values area).  Returns whether a TMA
-// copy was issued on `bar`.
-template <typename K, typename V, typename Src>
-__device__ __forceinline__ bool rbk_issue_reload(const Src &src, const RbkTile<K, V> &tl, const V *slot,
-                                                 unsigned char *buf, uint64_t *bar, uint64_t policy) {
-  using C = RbkCfg<K, V>;
-  constexpr uint32_t KC = 16 / sizeof(K);
-  if (!tl.tma) return false;
-  const uint32_t count = tl.count();
-  K *sk = reinterpret_cast<K *>(buf);
-  V *sv = reinterpret_cast<V *>(buf + C::KEY_BYTES);
-  if constexpr (Src::kSwz) {
-    mbar_arrive_expect_tx(bar, C::KROWS * 128u + (uint32_t)(C::TILE * sizeof(V)));
-    tma_load_rows(sk, src.key_map(), tl.local * C::KROWS, bar, policy);
-    tma_load_1d_hint(sv, slot, (uint32_t)(C::TILE * sizeof(V)), bar, policy);
-  } else {
-    const uint64_t base = (uint64_t)tl.local * C::TILE;
-    const uint32_t bk = count & ~(KC - 1);
-    for (uint32_t i = bk; i < count; ++i) sk[i] = tl.keys[base + i];
-    const uint32_t vbytes = (uint32_t)align_up(count * sizeof(V), 16);  // within the slot
-    mbar_arrive_expect_tx(bar, bk * (uint32_t)sizeof(K) + vbytes);
-    if (bk) tma_load_1d_hint(sk, tl.keys + base, bk * (uint32_t)sizeof(K), bar, policy);
-    tma_load_1d_hint(sv, slot, vbytes, bar, policy);
-  }
-  return true;
-}
-
 // Compute threads: plain copy of a tile into the buffer's layout (tiles
 // without a TMA copy).
 template <typename K, typename V, bool SWZ>
@@ -279,20 +260,6 @@ __device__ __forceinline__ void rbk_stage_load(const RbkTile<K, V> &tl, unsigned
     *reinterpret_cast<K *>(buf + area_off<SWZ>(i * (uint32_t)sizeof(K))) = tl.keys[base + i];
     *reinterpret_cast<V *>(buf + C::KEY_BYTES + area_off<SWZ>(i * (uint32_t)sizeof(V))) = tl.vals[base + i];
   }
-}
-
-// Compute threads: plain copy of a tile's keys and its mark slot (an image of
-// the values area) for phase 2.
-template <typename K, typename V, bool SWZ>
-__device__ __forceinline__ void rbk_stage_reload(const RbkTile<K, V> &tl, const V *slot, unsigned char *buf) {
-  using C = RbkCfg<K, V>;
-  const uint64_t base = (uint64_t)tl.local * C::TILE;
-  const uint32_t count = tl.count();
-  for (uint32_t i = threadIdx.x; i < count; i += kRbkWarps * 32)
-    *reinterpret_cast<K *>(buf + area_off<SWZ>(i * (uint32_t)sizeof(K))) = tl.keys[base + i];
-  const uint4 *s = reinterpret_cast<const uint4 *>(slot);
-  uint4 *d = reinterpret_cast<uint4 *>(buf + C::KEY_BYTES);
-  for (uint32_t c = threadIdx.x; c < (uint32_t)(C::TILE * sizeof(V) / 16); c += kRbkWarps * 32) d[c] = s[c];
 }
 
 // Loads a lane's B bytes (B = 32 or 64: C = B/16 chunks of 16 bytes) starting
@@ -346,21 +313,23 @@ struct LaneOffsets {
 // e0): loads them, flags run heads (a head's key differs from its
 // predecessor's; the input's first element is one), folds (c, v) in order --
 // c counts heads, v is the sum since the last head (or since the lane's first
-// element) -- and leaves the running v of every element in vals[] (the
-// "marks": at a run's last element, the run's sum from its head or from the
-// lane's start).  Returns (c, v); *heads / *tails get the head and tail bit
-// masks (bit j: element j starts / ends a run).  Elements past the tile's
-// end (FULL = false) are neither heads nor tails and add nothing.
+// element) -- and writes the running v of every element over its value in the
+// buffer (at a run's last element: the run's sum from its head or from the
+// lane's start; only this lane reads its values).  Returns (c, v); *heads /
+// *tails get the head and tail bit masks (bit j: element j starts / ends a
+// run).  Elements past the tile's end (FULL = false) are neither heads nor
+// tails and add nothing.
 template <typename K, typename V, bool SWZ, bool FULL>
-__device__ __forceinline__ Seg<V> rbk_phase1_lane(const unsigned char *buf, const LaneOffsets<K, V, SWZ> &lo,
+__device__ __forceinline__ Seg<V> rbk_phase1_lane(unsigned char *buf, const LaneOffsets<K, V, SWZ> &lo,
                                                   const K (*hb)[16 / sizeof(K)], uint32_t count, bool first_tile,
-                                                  bool last_tile, uint32_t e0, int lane, V (&val)[RbkCfg<K, V>::M],
-                                                  uint32_t *heads_out, uint32_t *tails_out) {
+                                                  bool last_tile, uint32_t e0, int lane, uint32_t *heads_out,
+                                                  uint32_t *tails_out) {
   using C = RbkCfg<K, V>;
   constexpr int M = C::M;
   constexpr int KC = 16 / sizeof(K);
   constexpr int VC = 16 / sizeof(V);
   K key[M];
+  V val[M];
   if constexpr (SWZ) {
 #pragma unroll
     for (int c = 0; c < C::KCH; ++c) {
@@ -421,35 +390,62 @@ __device__ __forceinline__ Seg<V> rbk_phase1_lane(const unsigned char *buf, cons
     tails = ((heads >> 1) & ((1u << (nvalid - 1)) - 1u)) |
             ((uint32_t)(last_tile || !(hb[1][0] == kl)) << (nvalid - 1));
   }
+  // the running values over the lane's values (the swizzled chunks of its
+  // loads; linear ones for batch tiles)
+#pragma unroll
+  for (int c = 0; c < C::VCH; ++c) {
+    uint4 q;
+    memcpy(&q, &val[c * VC], 16);
+    *reinterpret_cast<uint4 *>(buf + C::KEY_BYTES + (SWZ ? lo.v[c] : e0 * (uint32_t)sizeof(V) + 16u * c)) = q;
+  }
   *heads_out = heads;
   *tails_out = tails;
   return Seg<V>{(uint32_t)__popc(heads), v};
 }
 
-// Persistent two-phase reduce_by_key; the roles, buffer rotation and
-// hand-over protocol are scan_kernel's (scan.cu), with these differences: a
-// buffer holds a tile's keys, values and halo keys; phase 1 also writes every
-// element's running value (from its run's head, or from its lane's first
-// element) to the CTA's mark slot for the tile (ring slot blockIdx.x * 3 +
-// iteration mod 3, an image of the values area), and the re-read for phase 2
-// brings back the tile's keys with those marks in place of its values, so
-// phase 2 costs one step per run, not per element; phase 2 only reads its
-// buffer (the runs go straight to out_keys / out_vals), so the loader reuses
-// a buffer once the compute warps are done reading it, with no store to
-// drain; and tiles without a TMA copy are staged by the compute warps
-// themselves between two compute-only barriers.  Barrier phase parities are
-// kept as bit masks (bit b: buffer b), so no per-buffer array is indexed at
-// run time.
+// Persistent single-pass reduce_by_key.  Warps 0-7 compute, warp 8 (lane 0)
+// loads, warp 9 looks back.  Each CTA loops over tiles taken from an atomic
+// ticket (fetched one iteration ahead).  Tile t_i, ticketed for iteration i,
+// lives in buffer i mod NB and goes through:
+//   iteration i-D  loader: TMA copy of its keys, values and halo keys (tiles
+//                  without one -- the ragged end, or arrays not 16-byte
+//                  aligned -- are staged by the compute warps in iteration i);
+//   iteration i    compute: phase 1 -- each lane folds its M elements,
+//                  leaving their running sums over their values, and the
+//                  warps scan their lanes; after the compute warps' barrier
+//                  warp 7 publishes the tile aggregate and queues the tile
+//                  for the look-back warp, and each lane writes the runs
+//                  that end in its elements (the key, and the run's sum from
+//                  its head or from the tile's start) to the tile's run slot
+//                  (ring slot i mod 4 of the CTA) at their places in the
+//                  tile's output order; then the buffer is released;
+//   iteration i+3  compute: phase 2 -- with the tile's exclusive prefix
+//                  (c, v) from the look-back warp, the runs are copied from
+//                  the run slot to the output slots from c + h0 - 1 on (h0:
+//                  the tile starts a run), the first one adding v when it
+//                  began in an earlier tile.
+// The roles never share a barrier: they hand over through mbarriers.  full[b]:
+// the loader completes one phase per use of buffer b (a TMA copy, or a plain
+// arrival when there is nothing to copy) after writing the buffer's ticket;
+// empty[b]: each compute warp arrives when it is done with buffer b; qbar[e]:
+// the look-back warp hands over queue entry e's prefix.  The compute warps
+// meet only each other, once per iteration (after phase 1's reads), in a
+// barrier that also ORs their failure flags, so they all stop together; it
+// also orders an iteration's run-slot writes before the phase 2 that reads
+// them (whose first loads are issued at the start of its iteration, before
+// phase 1) and the phase 2 reads before the slot's next writes.  Every wait is
+// bounded by spin_limit_ns and gives up at once when anyone in the CTA has
+// failed.  Barrier phase parities are kept as bit masks (bit b: buffer b), so
+// no per-buffer array is indexed at run time.
 template <typename K, typename V, typename Src>
 __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_constant__ Src src,
                                                              typename RbkCfg<K, V>::Status st, WsHeader *hdr,
-                                                             V *ring, unsigned long long spin_limit_ns,
+                                                             unsigned char *ring, unsigned long long spin_limit_ns,
                                                              long long skip_publish_tile, unsigned int num_tiles) {
   using C = RbkCfg<K, V>;
   using P = typename C::P;
   constexpr bool SWZ = Src::kSwz;
-  constexpr int M = C::M, TILE = C::TILE, NB = kRbkBufs, Q = kRbkQueue;
-  V *const cta_ring = ring + (size_t)blockIdx.x * 3 * TILE;  // this CTA's three mark slots
+  constexpr int M = C::M, TILE = C::TILE, NB = C::NB, D = C::D, Q = kRbkQueue;
   constexpr unsigned int NONE = 0xffffffffu;
   OpSeg<V> op;
   extern __shared__ __align__(128) unsigned char smem_dyn[];
@@ -457,18 +453,15 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
   unsigned char *const smem_raw = smem_dyn + ((1024u - (smem_addr(smem_dyn) & 1023u)) & 1023u);
   __shared__ __align__(16) K s_halo[NB][2][16 / sizeof(K)];
   __shared__ __align__(8) uint64_t s_full[NB];
-  __shared__ __align__(8) uint64_t s_p1[NB];
-  __shared__ __align__(8) uint64_t s_p2[NB];
+  __shared__ __align__(8) uint64_t s_empty[NB];
   __shared__ __align__(8) uint64_t s_qbar[Q];
   __shared__ unsigned int s_ticket[NB];
-  __shared__ P s_wagg[4][kRbkWarps];   // per-warp (c, v) of t_i, by iteration mod 4
-  __shared__ P s_wexcl[4][kRbkWarps];  // the warps before each warp, folded (thread 0)
-  // phase 1's per-lane results, kept for phase 2 (each warp reads back only
-  // its own lanes, so program order protects them; by iteration mod 3):
-  // head flags | tail flags << 16, and the lane's exclusive (c, v) in its warp
-  __shared__ uint32_t s_lflags[3][32 * kRbkWarps];
-  __shared__ uint32_t s_lc[3][32 * kRbkWarps];
-  __shared__ V s_lv[3][32 * kRbkWarps];
+  // per tile, by iteration mod 2 (written in phase 1, read after the barrier
+  // that follows it): each warp's (c, v) and run count, and whether the tile
+  // starts with a head
+  __shared__ P s_wagg[2][kRbkWarps];
+  __shared__ uint32_t s_wruns[2][kRbkWarps];
+  __shared__ uint32_t s_h0[2];
   __shared__ unsigned int s_q_tile[Q];
   __shared__ P s_q_agg[Q];
   __shared__ P s_q_prefix[Q];
@@ -478,85 +471,82 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
   auto abort_now = [&]() { *reinterpret_cast<volatile int *>(&s_abort) = 1; };
   auto aborted = [&]() -> bool { return *reinterpret_cast<volatile int *>(&s_abort) != 0; };
   auto buf = [&](int b) { return smem_raw + (size_t)b * C::BUF_BYTES; };
-  auto slot = [&](int s) { return cta_ring + (size_t)s * TILE; };
+  // run slot s of this CTA: TILE keys, then TILE values
+  unsigned char *const cta_ring = ring + (size_t)blockIdx.x * kRbkRunSlots * C::RUN_SLOT_BYTES;
+  auto slot_keys = [&](int s) { return reinterpret_cast<K *>(cta_ring + (size_t)s * C::RUN_SLOT_BYTES); };
+  auto slot_vals = [&](int s) {
+    return reinterpret_cast<V *>(cta_ring + (size_t)s * C::RUN_SLOT_BYTES + sizeof(K) * TILE);
+  };
 
-  uint64_t keep = 0, stream = 0;
+  uint64_t stream = 0;
   uint32_t armpar = 0u, armany = 0u;  // loader: parity of the phases armed on s_full[b] / any armed
   unsigned int next_raw = NONE;
-  unsigned int t_first = NONE;
+  bool loads_done = false;
   if (tid == 32 * kRbkWarps) {
-    keep = l2_policy_evict_last();
     stream = l2_policy_evict_first();
     for (int b = 0; b < NB; ++b) {
       mbar_init(&s_full[b], 1);
-      mbar_init(&s_p1[b], kRbkWarps);
-      mbar_init(&s_p2[b], kRbkWarps);
+      mbar_init(&s_empty[b], kRbkWarps);
     }
     for (int q = 0; q < Q; ++q) mbar_init(&s_qbar[q], 1);
     fence_proxy_async_smem();
     s_abort = 0;
     s_q_in = 0u;
-    const unsigned int t0 = atomicAdd(&hdr->tile_ticket, 1u);
-    t_first = t0 < num_tiles ? t0 : NONE;
-    s_ticket[0] = t_first;
-    bool tx = false;
-    if (t_first != NONE) tx = rbk_issue_load<K, V>(src, src.tile(t_first), buf(0), s_halo[0], &s_full[0], keep);
-    if (!tx) mbar_arrive(&s_full[0]);
-    mbar_arrive(&s_full[NB - 1]);  // iteration 0's phase 2 reads buffer NB - 1: an empty phase
-    armpar = 1u | (1u << (NB - 1));
-    armany = armpar;
-    if (t_first != NONE) next_raw = atomicAdd(&hdr->tile_ticket, 1u);
+    // the loads of iterations 0 .. D-1 (tickets in order; none after the first past the end)
+    for (int d = 0; d < D; ++d) {
+      unsigned int tk = NONE;
+      if (!loads_done) {
+        tk = atomicAdd(&hdr->tile_ticket, 1u);
+        if (tk >= num_tiles) tk = NONE;
+      }
+      s_ticket[d] = tk;
+      bool tx = false;
+      if (tk != NONE) tx = rbk_issue_load<K, V>(src, src.tile(tk), buf(d), s_halo[d], &s_full[d], stream);
+      if (!tx) mbar_arrive(&s_full[d]);
+      armpar ^= 1u << d;
+      armany |= 1u << d;
+      if (tk == NONE) loads_done = true;
+    }
+    if (!loads_done) next_raw = atomicAdd(&hdr->tile_ticket, 1u);
   }
   __syncthreads();
 
   if (warp == kRbkWarps) {
     // ================= the loader (lane 0) =================
     if (lane != 0) return;
-    uint32_t p1par = 0u, p2par = 0u;
-    unsigned int t = t_first, p_tile = NONE, q_tile = NONE;
-    for (int it = 0;; ++it) {
-      const int bt = it % NB, bp = (it + NB - 1) % NB, bn = (it + 1) % NB;
-      // prefetch t_{i+1} into bn (the compute warps finished reading it last iteration)
-      const unsigned int tn = (t != NONE && next_raw < num_tiles) ? next_raw : NONE;
+    uint32_t epar = 0u;
+    for (int it = 0; !loads_done; ++it) {
+      // the load for iteration it + D goes to the buffer of iteration it - 1,
+      // free once that iteration's phase 1 is done with it
+      const int bn = (it + D) % NB;
+      if (it >= 1) {
+        if (!mbar_wait_or_abort(&s_empty[bn], (epar >> bn) & 1u, spin_limit_ns, &s_abort)) {
+          record_error(hdr, BK_ERR_SPIN_TIMEOUT, NONE);
+          abort_now();
+          break;
+        }
+        epar ^= 1u << bn;
+      }
+      const unsigned int tn = next_raw < num_tiles ? next_raw : NONE;
       s_ticket[bn] = tn;
       bool tx = false;
-      if (tn != NONE) tx = rbk_issue_load<K, V>(src, src.tile(tn), buf(bn), s_halo[bn], &s_full[bn], keep);
+      if (tn != NONE) tx = rbk_issue_load<K, V>(src, src.tile(tn), buf(bn), s_halo[bn], &s_full[bn], stream);
       if (!tx) mbar_arrive(&s_full[bn]);
       armpar ^= 1u << bn;
       armany |= 1u << bn;
-      next_raw = (tn != NONE) ? atomicAdd(&hdr->tile_ticket, 1u) : NONE;
-      // tiles are ticketed about in order, gridDim.x per iteration: ask L2 now
-      // for the one some CTA will load 1 iteration(s) from now
-      if (tn != NONE && tn + 1u * gridDim.x < num_tiles) {
-        const RbkTile<K, V> f = src.tile(tn + 1u * gridDim.x);
-        const uint64_t fb = (uint64_t)f.local * TILE;
-        prefetch_l2_range(f.keys + fb, (uint64_t)f.count() * sizeof(K));
-        prefetch_l2_range(f.vals + fb, (uint64_t)f.count() * sizeof(V));
+      if (tn == NONE) {
+        loads_done = true;
+      } else {
+        next_raw = atomicAdd(&hdr->tile_ticket, 1u);
+        // tiles are ticketed about in order, gridDim.x per iteration: ask L2
+        // now for the one some CTA will load an iteration from now
+        if (tn + gridDim.x < num_tiles) {
+          const RbkTile<K, V> f = src.tile(tn + gridDim.x);
+          const uint64_t fb = (uint64_t)f.local * TILE;
+          prefetch_l2_range(f.keys + fb, (uint64_t)f.count() * sizeof(K));
+          prefetch_l2_range(f.vals + fb, (uint64_t)f.count() * sizeof(V));
+        }
       }
-      // re-read t_{i-1} into t's buffer once phase 1 of t is done with it
-      if (!mbar_wait_or_abort(&s_p1[bt], (p1par >> bt) & 1u, spin_limit_ns, &s_abort)) {
-        record_error(hdr, BK_ERR_SPIN_TIMEOUT, t);
-        abort_now();
-        break;
-      }
-      p1par ^= 1u << bt;
-      tx = false;
-      if (q_tile != NONE)  // t_{it-1}: its phase 1 ran in iteration it-1
-        tx = rbk_issue_reload<K, V>(src, src.tile(q_tile), slot((it + 2) % 3), buf(bt), &s_full[bt], stream);
-      if (!tx) mbar_arrive(&s_full[bt]);
-      armpar ^= 1u << bt;
-      armany |= 1u << bt;
-      // buffer bp is free once phase 2 of p has read it
-      if (!mbar_wait_or_abort(&s_p2[bp], (p2par >> bp) & 1u, spin_limit_ns, &s_abort)) {
-        record_error(hdr, BK_ERR_SPIN_TIMEOUT, p_tile);
-        abort_now();
-        break;
-      }
-      p2par ^= 1u << bp;
-      p_tile = q_tile;
-      q_tile = t;
-      t = tn;
-      if (t == NONE && p_tile == NONE && q_tile == NONE) break;
     }
     // every load must land before the CTA's shared memory goes away: wait for
     // the last phase armed on each buffer (phases of a barrier complete in order)
@@ -591,6 +581,10 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
       }
       return __all_sync(0xffffffffu, ready);
     };
+    // tiles in queue order, each once the next one is queued (its
+    // predecessors have then had an iteration to publish; its phase 2 is
+    // three iterations after its phase 1), so the L2 round trips of the
+    // look-back mostly find aggregates and prefixes already there
     for (unsigned int j = 0;; ++j) {
       if (!wait_queued(j + 1u)) break;
       const unsigned int q = s_q_tile[j % Q];
@@ -619,124 +613,192 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
   const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;  // this lane's first element in every tile
   const LaneOffsets<K, V, SWZ> lo(e0);
   uint32_t fpar = 0u;  // bit b: parity of the next phase of s_full[b]
-  unsigned int p_tile = NONE, q_tile = NONE;
+  // the tiles of the last three iterations (index: iterations ago - 1), their
+  // run counts, whether they start with a head, and their head counts
+  unsigned int tq[3] = {NONE, NONE, NONE};
+  uint32_t rq[3] = {0u, 0u, 0u}, hq[3] = {0u, 0u, 0u}, cq[3] = {0u, 0u, 0u};
+  bool ended = false;                 // an iteration has had no tile: no more loads
   bool bad = false;
 
   for (int it = 0;; ++it) {
-    const int bt = it % NB, bp = (it + NB - 1) % NB;
-    const unsigned int p = p_tile;
+    const int bt = it % NB, ps = it & 1;
+    const unsigned int p = tq[2];  // phase 2 of t_{it-3}
+    const uint32_t pr = rq[2], ph = hq[2], pc = cq[2];
+
+    // phase 2 of p reads its run slot (written before the last barrier):
+    // start the loads of this thread's first two runs now, so that their L2
+    // round trip overlaps phase 1
+    K pk[2];
+    V pv[2];
+    if (p != NONE) {
+      const K *const rk = slot_keys((it + 1) % kRbkRunSlots);  // == (it - 3) mod 4
+      const V *const rv = slot_vals((it + 1) % kRbkRunSlots);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const uint32_t i = (uint32_t)tid + 32u * kRbkWarps * k;
+        if (i < pr) {
+          pk[k] = rk[i];
+          pv[k] = rv[i];
+        }
+      }
+    }
 
     // ---- phase 1 of t
     unsigned int t = NONE;
-    if (!mbar_wait_or_abort(&s_full[bt], (fpar >> bt) & 1u, spin_limit_ns, &s_abort)) bad = true;
-    fpar ^= 1u << bt;
-    // the marks this thread stored last iteration are read back by a TMA copy
-    // that the loader issues once this iteration's phase 1 is done: order them
-    // before it now, an iteration after the stores (fencing right after them
-    // would wait for their round trip to L2)
-    fence_proxy_async_global();
-    bad = __any_sync(0xffffffffu, bad);
-    if (!bad) t = s_ticket[bt];
-    // tiles without a TMA copy: the compute warps stage them here, between
-    // two barriers that every compute warp takes whenever the launch may
-    // have such a tile (a flag of the launch, so a warp that saw a failure
-    // still takes part; the previous iteration's readers are past the first)
-    if (src.may_stage) {
-      named_barrier_sync(2, 32 * kRbkWarps);
-      if (t != NONE && !src.tile(t).tma) rbk_stage_load<K, V, SWZ>(src.tile(t), buf(bt));
-      if (p != NONE && !bad && !src.tile(p).tma)  // phase 1 of p ran at it - 2
-        rbk_stage_reload<K, V, SWZ>(src.tile(p), slot((it + 1) % 3), buf(bp));
-      named_barrier_sync(2, 32 * kRbkWarps);
+    if (!ended) {
+      if (!mbar_wait_or_abort(&s_full[bt], (fpar >> bt) & 1u, spin_limit_ns, &s_abort)) bad = true;
+      fpar ^= 1u << bt;
+      bad = __any_sync(0xffffffffu, bad);
+      if (!bad) t = s_ticket[bt];
+      // tiles without a TMA copy: the compute warps stage them here, then meet
+      // (every compute warp takes that barrier whenever the launch may have
+      // such a tile -- a flag of the launch, so a warp that saw a failure
+      // still takes part; the buffer's previous tile was done with it before
+      // the last iteration's barrier)
+      if (src.may_stage) {
+        if (t != NONE && !src.tile(t).tma) {
+          rbk_stage_load<K, V, SWZ>(src.tile(t), buf(bt));
+          fence_proxy_async_smem();  // as after phase 1's own stores below
+        }
+        named_barrier_sync(2, 32 * kRbkWarps);
+      }
     }
+    uint32_t heads = 0u, tails = 0u;
+    P lex = OpSeg<V>::identity();  // the lane's exclusive (c, v) within its warp
     if (t != NONE) {
       const RbkTile<K, V> tl = src.tile(t);
       const uint32_t count = tl.count();
-      V val[M];
-      uint32_t heads, tails;
       P lane_agg;
       if (count == (uint32_t)TILE)  // every tile but an array's last: no bounds checks
         lane_agg = rbk_phase1_lane<K, V, SWZ, true>(buf(bt), lo, s_halo[bt], count, tl.first(), tl.last(), e0, lane,
-                                                    val, &heads, &tails);
+                                                    &heads, &tails);
       else
         lane_agg = rbk_phase1_lane<K, V, SWZ, false>(buf(bt), lo, s_halo[bt], count, tl.first(), tl.last(), e0,
-                                                     lane, val, &heads, &tails);
-      // the running values go to the tile's mark slot (an image of the values area)
-      unsigned char *const ms = reinterpret_cast<unsigned char *>(slot(it % 3));
-#pragma unroll
-      for (int c = 0; c < C::VCH; ++c) {
-        uint4 q;
-        memcpy(&q, &val[c * (16 / sizeof(V))], 16);
-        *reinterpret_cast<uint4 *>(ms + (SWZ ? lo.v[c] : e0 * (uint32_t)sizeof(V) + 16u * c)) = q;
-      }
+                                                     lane, &heads, &tails);
       const P incl = warp_inclusive_scan(lane_agg, op, lane);
-      if (lane == 31) s_wagg[it & 3][warp] = incl;
-      P lex = shfl_up(incl, 1);
-      if (lane == 0) lex = OpSeg<V>::identity();
-      const int sl = it % 3, li = warp * 32 + lane;
-      s_lflags[sl][li] = heads | (tails << 16);
-      s_lc[sl][li] = lex.c;
-      s_lv[sl][li] = lex.v;
-    }
-    __syncwarp();
-    if (!bad && lane == 0) mbar_arrive(&s_p1[bt]);
-    if (named_barrier_or(1, 32 * kRbkWarps, bad || aborted())) break;
-
-    // ---- thread 0: publish t's aggregate and queue t for the look-back
-    if (tid == 0) {
-      P agg = OpSeg<V>::identity();
-      if (t != NONE) {
-#pragma unroll
-        for (int i = 0; i < kRbkWarps; ++i) {
-          s_wexcl[it & 3][i] = agg;
-          agg = op(agg, s_wagg[it & 3][i]);
-        }
-        if ((long long)t != skip_publish_tile) st.publish(t, src.tile(t).first() ? kStPrefix : kStAggregate, agg);
+      const uint32_t nr = __reduce_add_sync(0xffffffffu, (uint32_t)__popc(tails));
+      if (lane == 31) {
+        s_wagg[ps][warp] = incl;
+        s_wruns[ps][warp] = nr;
       }
-      s_q_tile[it % Q] = t;
-      s_q_agg[it % Q] = agg;
+      lex = shfl_up(incl, 1);
+      if (lane == 0) lex = OpSeg<V>::identity();
+      if (tid == 0) s_h0[ps] = heads & 1u;
+    }
+    if (named_barrier_or(1, 32 * kRbkWarps, bad || aborted())) {
+      if (lane == 0) abort_now();  // the loader and the look-back warp stop too
+      break;
+    }
+
+    uint32_t h0 = 0u, nruns = 0u, aggc = 0u;
+    if (t != NONE) {
+      h0 = s_h0[ps];
+      // lanes 0-7 scan the warps' (c, v) and run counts: lane w - 1 then holds
+      // the fold of warps 0 .. w-1, lane 7 the tile's
+      P a = OpSeg<V>::identity();
+      uint32_t rc = 0u;
+      if (lane < kRbkWarps) {
+        a = s_wagg[ps][lane];
+        rc = s_wruns[ps][lane];
+      }
+#pragma unroll
+      for (int d = 1; d < kRbkWarps; d <<= 1) {
+        const P o = shfl_up(a, d);
+        const uint32_t ro = __shfl_up_sync(0xffffffffu, rc, d);
+        if (lane >= d) {
+          a = op(o, a);
+          rc += ro;
+        }
+      }
+      P wex = shfl_idx_any(a, warp > 0 ? warp - 1 : 0);
+      if (warp == 0) wex = OpSeg<V>::identity();
+      const P agg = shfl_idx_any(a, kRbkWarps - 1);
+      nruns = __shfl_sync(0xffffffffu, rc, kRbkWarps - 1);
+      aggc = agg.c;
+      if (warp == kRbkWarps - 1 && lane == 0) {
+        if ((long long)t != skip_publish_tile) st.publish(t, src.tile(t).first() ? kStPrefix : kStAggregate, agg);
+        s_q_tile[it % Q] = t;
+        s_q_agg[it % Q] = agg;
+        st_release_cta_u32(&s_q_in, (unsigned int)it + 1u);
+      }
+      // the runs ending in this lane's elements go to the tile's run slot.
+      // A run's slot within the tile counts the tile's heads up to its tail,
+      // less h0; a lane's only head before its first tail can be its first
+      // element, and a first tail with no head before it closes a run that
+      // began before the lane, whose sum so far is the lane's exclusive v
+      // (later tails' running values start at a head of the lane).
+      if (tails != 0u) {
+        K *const rk = slot_keys(it % kRbkRunSlots);
+        V *const rv = slot_vals(it % kRbkRunSlots);
+        const unsigned char *const b = buf(bt);
+        const P lx = op(wex, lex);
+        uint32_t r = lx.c - h0 + (heads & 1u);
+        bool open = (heads & 1u) == 0u;
+        for (uint32_t tb = tails; tb != 0u; tb &= tb - 1u) {
+          const uint32_t e = e0 + (uint32_t)__ffs(tb) - 1u;
+          const K k = *reinterpret_cast<const K *>(b + area_off<SWZ>(e * (uint32_t)sizeof(K)));
+          V v = *reinterpret_cast<const V *>(b + C::KEY_BYTES + area_off<SWZ>(e * (uint32_t)sizeof(V)));
+          if (open) v = (V)(lx.v + v);
+          open = false;
+          rk[r] = k;
+          rv[r] = v;
+          ++r;
+        }
+      }
+      // the loader's next TMA copy into this buffer must land after phase 1's
+      // stores to it
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&s_empty[bt]);
+    } else if (!ended && warp == kRbkWarps - 1 && lane == 0) {
+      s_q_tile[it % Q] = NONE;  // ends the look-back warp's loop
       st_release_cta_u32(&s_q_in, (unsigned int)it + 1u);
     }
 
-    // ---- phase 2 of p: emit its runs
-    if (!mbar_wait_or_abort(&s_full[bp], (fpar >> bp) & 1u, spin_limit_ns, &s_abort)) bad = true;
-    fpar ^= 1u << bp;
-    if (p != NONE && !bad) {
-      const unsigned int e = (unsigned int)it - 2u;
+    // ---- phase 2 of p = t_{it-3}: its runs from its run slot to the output
+    if (p != NONE) {
+      const unsigned int e = (unsigned int)it - 3u;
       if (!mbar_wait_or_abort(&s_qbar[e % Q], (e / Q) & 1u, spin_limit_ns, &s_abort)) bad = true;
-    }
-    bad = __any_sync(0xffffffffu, bad);
-    if (p != NONE && !bad) {
-      const unsigned int e = (unsigned int)it - 2u;
-      const RbkTile<K, V> tl = src.tile(p);
-      const uint32_t count = tl.count();
-      const int sl = (it + 1) % 3, li = warp * 32 + lane;  // phase 1 of p ran at it - 2
-      const uint32_t fl = s_lflags[sl][li];
-      const uint32_t head = fl & 0xffffu, tail = fl >> 16;
-      const bool holds_last = tl.last() && e0 < count && count <= e0 + M;  // the input's last element
-      if (tail != 0u || holds_last) {
-        P carry = op(s_q_prefix[e % Q], s_wexcl[(it + 2) & 3][warp]);
-        carry = op(carry, P{s_lc[sl][li], s_lv[sl][li]});
-        // each tail: its key, and its mark (the run's value from its head, or
-        // from the lane's first element when the run began before the lane)
-        const unsigned char *bP = buf(bp);
-        for (uint32_t tb = tail; tb != 0u; tb &= tb - 1u) {
-          const uint32_t j = (uint32_t)__ffs(tb) - 1u;
-          const uint32_t upto = head & ((2u << j) - 1u);  // heads at or before j
-          const uint32_t c = carry.c + (uint32_t)__popc(upto);
-          V v = *reinterpret_cast<const V *>(bP + C::KEY_BYTES + area_off<SWZ>((e0 + j) * (uint32_t)sizeof(V)));
-          if (upto == 0u) v = (V)(carry.v + v);
-          tl.out_keys[c - 1] = *reinterpret_cast<const K *>(bP + area_off<SWZ>((e0 + j) * (uint32_t)sizeof(K)));
-          tl.out_vals[c - 1] = v;
+      bad = __any_sync(0xffffffffu, bad);
+      if (!bad) {
+        const RbkTile<K, V> tl = src.tile(p);
+        const P pre = s_q_prefix[e % Q];
+        // the tile's first run goes to slot pre.c + h0 - 1 (pre.c >= 1 when h0 = 0)
+        K *const ok = tl.out_keys + ((uint64_t)pre.c + ph - 1u);
+        V *const ov = tl.out_vals + ((uint64_t)pre.c + ph - 1u);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const uint32_t i = (uint32_t)tid + 32u * kRbkWarps * k;
+          if (i < pr) {
+            V v = pv[k];
+            if (i == 0u && ph == 0u) v = (V)(pre.v + v);
+            ok[i] = pk[k];
+            ov[i] = v;
+          }
         }
-        if (holds_last) *tl.num_out = carry.c + (uint32_t)__popc(head);
+        const K *const rk = slot_keys((int)(e % kRbkRunSlots));
+        const V *const rv = slot_vals((int)(e % kRbkRunSlots));
+        for (uint32_t i = (uint32_t)tid + 64u * kRbkWarps; i < pr; i += 32u * kRbkWarps) {
+          ok[i] = rk[i];
+          ov[i] = rv[i];
+        }
+        if (tid == 0 && tl.last()) *tl.num_out = (uint64_t)pre.c + pc;
       }
     }
-    __syncwarp();
-    if (!bad && lane == 0) mbar_arrive(&s_p2[bp]);
 
-    p_tile = q_tile;
-    q_tile = t;
-    if (t == NONE && p_tile == NONE && q_tile == NONE) break;
+    if (t == NONE) ended = true;
+#pragma unroll
+    for (int k = 2; k > 0; --k) {
+      tq[k] = tq[k - 1];
+      rq[k] = rq[k - 1];
+      hq[k] = hq[k - 1];
+      cq[k] = cq[k - 1];
+    }
+    tq[0] = t;
+    rq[0] = nruns;
+    hq[0] = h0;
+    cq[0] = aggc;
+    if (t == NONE && tq[1] == NONE && tq[2] == NONE) break;
   }
 }
 
@@ -758,14 +820,14 @@ int rbk_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStrea
   if ((st = host::launch_status()) != BK_OK) return st;
   const host::DebugFault dbg = host::debug_fault();
   const unsigned long long limit = dbg.spin_limit_ns ? dbg.spin_limit_ns : host::kDefaultSpinLimitNs;
-  const size_t smem = (size_t)kRbkBufs * C::BUF_BYTES + 1024;  // + room to align the buffers to 1024 bytes
+  const size_t smem = (size_t)C::NB * C::BUF_BYTES + 1024;  // + room to align the buffers to 1024 bytes
   struct Site {};
   host::KernelSetup ks;
   if ((st = host::kernel_setup<Site>(rbk_kernel<K, V, Src>, kRbkThreads, smem, &ks)) != BK_OK) return st;
   const tune::Knobs kn = tune::knobs_for(tune::kReduceByKey, (int)(sizeof(K) + sizeof(V)), (uint64_t)tiles * C::TILE);
   const size_t per_sm = (size_t)std::min(std::max(kn.ctas_per_sm, 1), 2);
   const unsigned grid = (unsigned)std::min<size_t>(tiles, std::min<size_t>((size_t)di.sm_count * per_sm, kRbkMaxGrid));
-  V *ring = reinterpret_cast<V *>(reinterpret_cast<char *>(d_ws) + rbk_ring_offset<K, V>(tiles));
+  unsigned char *ring = reinterpret_cast<unsigned char *>(d_ws) + rbk_ring_offset<K, V>(tiles);
   rbk_kernel<K, V, Src><<<grid, kRbkThreads, smem, stream>>>(src, status, hdr, ring, limit, dbg.skip_publish_tile,
                                                             (unsigned)tiles);
   return host::launch_status();
