@@ -58,24 +58,32 @@ constexpr int kRbkQueue = 4;                       // look-back queue entries
 
 template <typename K, typename V>
 struct RbkCfg {
-  // each lane owns M consecutive elements: 64 bytes of the wider of key/value
-  static constexpr int M = 64 / (sizeof(K) > sizeof(V) ? sizeof(K) : sizeof(V));  // 16 or 8
-  static constexpr int TILE = kRbkWarps * 32 * M;                                  // 4096 or 2048
-  static constexpr uint32_t KROWS = sizeof(K) * TILE / 128;  // 128-byte rows of keys in a tile
+  // each lane owns M consecutive elements and reads them in passes of MP (64
+  // bytes of the wider of key and value, so that a pass's keys and values fit
+  // in registers).  A tile's fixed costs -- the barrier, the publication, the
+  // look-back -- are paid once per tile, so tiles are as large as two CTAs
+  // per SM allow: 16 elements a lane (two passes when one of key and value is
+  // 8 bytes wide), or 8 when both are.  Wider lanes of 4-byte pairs (24
+  // elements, 96 bytes apart) measured slower: their chunks meet in the
+  // shared-memory banks.
+  static constexpr int M = sizeof(K) + sizeof(V) <= 12 ? 16 : 8;
+  static constexpr int MP = 64 / (sizeof(K) > sizeof(V) ? sizeof(K) : sizeof(V));  // 16 or 8
+  static_assert(M % MP == 0, "whole passes");
+  static constexpr int TILE = kRbkWarps * 32 * M;            // 4096 or 2048
+  static constexpr uint32_t KROWS = sizeof(K) * TILE / 128;  // 128-byte rows of keys in a tile (<= 256)
   static constexpr uint32_t VROWS = sizeof(V) * TILE / 128;  // ... and of values
   // a buffer: the keys area, then the values area, each a whole number of
-  // 1024-byte swizzle periods
+  // 1024-byte swizzle periods (32 or 48 KB)
   static constexpr size_t KEY_BYTES = align_up(sizeof(K) * TILE, 1024);
   static constexpr size_t VAL_BYTES = align_up(sizeof(V) * TILE, 1024);
   static constexpr size_t BUF_BYTES = KEY_BYTES + VAL_BYTES;
   // tile buffers in rotation: a tile holds one from its load, D iterations
   // before its phase 1, to the end of its phase 1, so NB = D + 1; two CTAs per
   // SM keep NB * BUF_BYTES under half the SM's shared memory
-  static constexpr int NB = BUF_BYTES <= 24 * 1024 ? 4 : 3;
+  static constexpr int NB = BUF_BYTES <= 32 * 1024 ? 3 : 2;
+  static_assert(NB * BUF_BYTES <= 100 * 1024, "two CTAs per SM");
   static constexpr int D = NB - 1;
   static constexpr size_t RUN_SLOT_BYTES = (sizeof(K) + sizeof(V)) * TILE;  // a tile's runs, at most TILE
-  static constexpr int KCH = M * (int)sizeof(K) / 16;  // 16-byte chunks of a lane's keys
-  static constexpr int VCH = M * (int)sizeof(V) / 16;  // ... and of its values
   using P = Seg<V>;
   using Status = TileStatus<P>;
 };
@@ -262,18 +270,25 @@ __device__ __forceinline__ void rbk_stage_load(const RbkTile<K, V> &tl, unsigned
   }
 }
 
-// Loads a lane's B bytes (B = 32 or 64: C = B/16 chunks of 16 bytes) starting
-// at byte offset lane_off of a linear area into dst, conflict-free: eight
-// lanes share one 128-byte bank period, so lane l fetches its chunks starting
-// at chunk r = (l / (8 / C)) mod C, which gives the eight lanes of every
-// access phase distinct banks; two select stages then rotate the chunks back
-// into order.  (Used for tiles of a batch, which arrive unswizzled.)
+// Loads a lane's B bytes (C = B/16 chunks of 16 bytes, one to eight) starting
+// at byte offset lane_off of a linear area into dst.  For two or four chunks,
+// lane l fetches its chunks starting at chunk r = (l / (8 / C)) mod C, which
+// spreads the eight lanes of an access phase over the banks when lanes are B
+// bytes apart (and halves the conflicts when they are 2B apart); two select
+// stages then rotate the chunks back into order.  Other counts load in order.
+// (Used for tiles of a batch, which arrive unswizzled.)
 template <int B, typename T>
 __device__ __forceinline__ void load_lane_rotated(T *dst, const unsigned char *base, uint32_t lane_off, int lane) {
   constexpr int C = B / 16;
-  static_assert(C == 2 || C == 4, "two or four 16-byte chunks");
-  const int r = (lane / (8 / C)) & (C - 1);
+  static_assert(C >= 1 && C <= 8, "one to eight 16-byte chunks");
   uint4 q[C];
+  if constexpr (C != 2 && C != 4) {  // no rotation: chunks in order
+#pragma unroll
+    for (int k = 0; k < C; ++k) q[k] = *reinterpret_cast<const uint4 *>(base + lane_off + 16 * k);
+    memcpy(dst, q, B);
+    return;
+  }
+  const int r = (lane / (8 / C)) & (C - 1);
 #pragma unroll
   for (int k = 0; k < C; ++k) q[k] = *reinterpret_cast<const uint4 *>(base + lane_off + 16 * ((k + r) & (C - 1)));
   // q[k] holds chunk (k + r) mod C; rotate right by r so q[c] holds chunk c
@@ -295,108 +310,107 @@ __device__ __forceinline__ void load_lane_rotated(T *dst, const unsigned char *b
   memcpy(dst, q, B);
 }
 
-// A lane's 16-byte chunk offsets within the keys and values areas (the same
-// for every tile: they depend on the lane's first element only).
-template <typename K, typename V, bool SWZ>
-struct LaneOffsets {
-  uint32_t k[RbkCfg<K, V>::KCH];
-  uint32_t v[RbkCfg<K, V>::VCH];
-  __device__ __forceinline__ explicit LaneOffsets(uint32_t e0) {
-#pragma unroll
-    for (int c = 0; c < RbkCfg<K, V>::KCH; ++c) k[c] = area_off<SWZ>(e0 * (uint32_t)sizeof(K) + 16u * c);
-#pragma unroll
-    for (int c = 0; c < RbkCfg<K, V>::VCH; ++c) v[c] = area_off<SWZ>(e0 * (uint32_t)sizeof(V) + 16u * c);
-  }
-};
-
 // Phase 1 of a lane's M consecutive elements (element index of its first:
-// e0): loads them, flags run heads (a head's key differs from its
-// predecessor's; the input's first element is one), folds (c, v) in order --
-// c counts heads, v is the sum since the last head (or since the lane's first
-// element) -- and writes the running v of every element over its value in the
-// buffer (at a run's last element: the run's sum from its head or from the
-// lane's start; only this lane reads its values).  Returns (c, v); *heads /
-// *tails get the head and tail bit masks (bit j: element j starts / ends a
-// run).  Elements past the tile's end (FULL = false) are neither heads nor
-// tails and add nothing.
+// e0), in passes of MP elements (so that one pass's keys and values fit in
+// registers): loads them, flags run
+// heads (a head's key differs from its predecessor's; the input's first
+// element is one), folds (c, v) in order -- c counts heads, v is the sum since
+// the last head (or since the lane's first element) -- and writes the running
+// v of every element over its value in the buffer (at a run's last element:
+// the run's sum from its head or from the lane's start; only this lane reads
+// its values).  Returns (c, v); *heads / *tails get the head and tail bit
+// masks (bit j: element j starts / ends a run).  Elements past the tile's end
+// (FULL = false) are neither heads nor tails and add nothing.  Whether the
+// lane's first element is a head is known only once the previous lane's last
+// key has been shuffled over, after the passes; the fold does not depend on
+// it (v starts at the first value either way).
 template <typename K, typename V, bool SWZ, bool FULL>
-__device__ __forceinline__ Seg<V> rbk_phase1_lane(unsigned char *buf, const LaneOffsets<K, V, SWZ> &lo,
-                                                  const K (*hb)[16 / sizeof(K)], uint32_t count, bool first_tile,
-                                                  bool last_tile, uint32_t e0, int lane, uint32_t *heads_out,
-                                                  uint32_t *tails_out) {
+__device__ __forceinline__ Seg<V> rbk_phase1_lane(unsigned char *buf, const K (*hb)[16 / sizeof(K)], uint32_t count,
+                                                  bool first_tile, bool last_tile, uint32_t e0, int lane,
+                                                  uint32_t *heads_out, uint32_t *tails_out) {
   using C = RbkCfg<K, V>;
-  constexpr int M = C::M;
+  constexpr int M = C::M, MP = C::MP;
   constexpr int KC = 16 / sizeof(K);
   constexpr int VC = 16 / sizeof(V);
-  K key[M];
-  V val[M];
-  if constexpr (SWZ) {
-#pragma unroll
-    for (int c = 0; c < C::KCH; ++c) {
-      const uint4 q = *reinterpret_cast<const uint4 *>(buf + lo.k[c]);
-      memcpy(&key[c * KC], &q, 16);
-    }
-#pragma unroll
-    for (int c = 0; c < C::VCH; ++c) {
-      const uint4 q = *reinterpret_cast<const uint4 *>(buf + C::KEY_BYTES + lo.v[c]);
-      memcpy(&val[c * VC], &q, 16);
-    }
-  } else {
-    load_lane_rotated<M * sizeof(K)>(key, buf, e0 * (uint32_t)sizeof(K), lane);
-    load_lane_rotated<M * sizeof(V)>(val, buf + C::KEY_BYTES, e0 * (uint32_t)sizeof(V), lane);
-  }
   const int nvalid = FULL ? M : (int)min(max((int)count - (int)e0, 0), M);
-  if (!FULL && nvalid < M) {
+  K kfirst = K(), klast = K(), pk = K();
+  V v = V(0);
+  uint32_t heads = 0;
 #pragma unroll
-    for (int j = 0; j < M; ++j)
-      if (j >= nvalid) {
-        key[j] = K();
-        val[j] = V(0);
+  for (int ps = 0; ps < M / MP; ++ps) {
+    K key[MP];
+    V val[MP];
+    const uint32_t kb = (e0 + ps * MP) * (uint32_t)sizeof(K);  // byte offsets of the pass
+    const uint32_t vb = (e0 + ps * MP) * (uint32_t)sizeof(V);
+    if constexpr (SWZ) {
+#pragma unroll
+      for (int c = 0; c < MP * (int)sizeof(K) / 16; ++c) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(buf + swz128(kb + 16u * c));
+        memcpy(&key[c * KC], &q, 16);
       }
+#pragma unroll
+      for (int c = 0; c < MP * (int)sizeof(V) / 16; ++c) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(buf + C::KEY_BYTES + swz128(vb + 16u * c));
+        memcpy(&val[c * VC], &q, 16);
+      }
+    } else {
+      load_lane_rotated<MP * sizeof(K)>(key, buf, kb, lane);
+      load_lane_rotated<MP * sizeof(V)>(val, buf + C::KEY_BYTES, vb, lane);
+    }
+    if (!FULL) {
+#pragma unroll
+      for (int j = 0; j < MP; ++j)
+        if (ps * MP + j >= nvalid) {
+          key[j] = K();
+          val[j] = V(0);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < MP; ++j) {
+      const int jj = ps * MP + j;
+      if (jj == 0) {
+        kfirst = key[0];
+        v = val[0];
+      } else {
+        bool h = !(key[j] == pk);
+        if (!FULL) h = h && (jj < nvalid);
+        v = h ? val[j] : (V)(v + val[j]);
+        heads |= (uint32_t)h << jj;
+      }
+      val[j] = v;
+      pk = key[j];
+      if (!FULL && jj == nvalid - 1) klast = key[j];
+    }
+    if (FULL) klast = key[MP - 1];
+    // the running values over the pass's values (the chunks it loaded)
+#pragma unroll
+    for (int c = 0; c < MP * (int)sizeof(V) / 16; ++c) {
+      uint4 q;
+      memcpy(&q, &val[c * VC], 16);
+      *reinterpret_cast<uint4 *>(buf + C::KEY_BYTES + (SWZ ? swz128(vb + 16u * c) : vb + 16u * c)) = q;
+    }
   }
-  // the key before the lane's first element and after its last
-  K prev = shfl_up(key[M - 1], 1);
-  K next = shfl_down_any(key[0], 1);
+  // the key before the lane's first element and after its last (a lane past
+  // the tile's end shuffles a zero key that nothing reads)
+  K prev = shfl_up(pk, 1);
+  K next = shfl_down_any(kfirst, 1);
   if (lane == 0)
     prev = e0 == 0 ? hb[0][KC - 1] : *reinterpret_cast<const K *>(buf + area_off<SWZ>((e0 - 1) * (uint32_t)sizeof(K)));
   if (lane == 31)
     next = e0 + M < count ? *reinterpret_cast<const K *>(buf + area_off<SWZ>((e0 + M) * (uint32_t)sizeof(K)))
                           : hb[1][0];
-  const bool force0 = first_tile && e0 == 0;
-  K pk = prev;
-  V v = V(0);
-  uint32_t heads = 0;
-#pragma unroll
-  for (int j = 0; j < M; ++j) {
-    bool h = !(key[j] == pk);
-    if (j == 0) h = h || force0;
-    if (!FULL) h = h && (j < nvalid);
-    v = h ? val[j] : (V)(v + val[j]);
-    val[j] = v;
-    heads |= (uint32_t)h << j;
-    pk = key[j];
-  }
+  bool h0 = !(kfirst == prev) || (first_tile && e0 == 0);
+  if (!FULL) h0 = h0 && nvalid > 0;
+  heads |= (uint32_t)h0;
   // element j < nvalid - 1 ends a run exactly when j + 1 starts one
   uint32_t tails = 0;
   if (nvalid == M) {
     const bool tile_end = e0 + M == count;
-    const bool tl = tile_end ? (last_tile || !(hb[1][0] == key[M - 1])) : !(next == key[M - 1]);
+    const bool tl = tile_end ? (last_tile || !(hb[1][0] == klast)) : !(next == klast);
     tails = (heads >> 1) | ((uint32_t)tl << (M - 1));
   } else if (nvalid > 0) {  // the lane holding the tile's last element
-    K kl = key[0];
-#pragma unroll
-    for (int j = 1; j < M; ++j)
-      if (j == nvalid - 1) kl = key[j];
     tails = ((heads >> 1) & ((1u << (nvalid - 1)) - 1u)) |
-            ((uint32_t)(last_tile || !(hb[1][0] == kl)) << (nvalid - 1));
-  }
-  // the running values over the lane's values (the swizzled chunks of its
-  // loads; linear ones for batch tiles)
-#pragma unroll
-  for (int c = 0; c < C::VCH; ++c) {
-    uint4 q;
-    memcpy(&q, &val[c * VC], 16);
-    *reinterpret_cast<uint4 *>(buf + C::KEY_BYTES + (SWZ ? lo.v[c] : e0 * (uint32_t)sizeof(V) + 16u * c)) = q;
+            ((uint32_t)(last_tile || !(hb[1][0] == klast)) << (nvalid - 1));
   }
   *heads_out = heads;
   *tails_out = tails;
@@ -611,7 +625,6 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
 
   // ================= the compute warps =================
   const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;  // this lane's first element in every tile
-  const LaneOffsets<K, V, SWZ> lo(e0);
   uint32_t fpar = 0u;  // bit b: parity of the next phase of s_full[b]
   // the tiles of the last three iterations (index: iterations ago - 1), their
   // run counts, whether they start with a head, and their head counts
@@ -670,11 +683,11 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
       const uint32_t count = tl.count();
       P lane_agg;
       if (count == (uint32_t)TILE)  // every tile but an array's last: no bounds checks
-        lane_agg = rbk_phase1_lane<K, V, SWZ, true>(buf(bt), lo, s_halo[bt], count, tl.first(), tl.last(), e0, lane,
+        lane_agg = rbk_phase1_lane<K, V, SWZ, true>(buf(bt), s_halo[bt], count, tl.first(), tl.last(), e0, lane,
                                                     &heads, &tails);
       else
-        lane_agg = rbk_phase1_lane<K, V, SWZ, false>(buf(bt), lo, s_halo[bt], count, tl.first(), tl.last(), e0,
-                                                     lane, &heads, &tails);
+        lane_agg = rbk_phase1_lane<K, V, SWZ, false>(buf(bt), s_halo[bt], count, tl.first(), tl.last(), e0, lane,
+                                                     &heads, &tails);
       const P incl = warp_inclusive_scan(lane_agg, op, lane);
       const uint32_t nr = __reduce_add_sync(0xffffffffu, (uint32_t)__popc(tails));
       if (lane == 31) {

@@ -64,12 +64,20 @@ def _vals(tag, n, seed):
     return oracle.gen(np.int32, n, seed, -1000, 1000).astype(NP[tag])
 
 
+def _tile(kt, vt):
+    """Elements per tile: 256 lanes x 16 elements (8 when key and value are both 8 bytes wide)."""
+    return 256 * (16 if NP[kt]().itemsize + NP[vt]().itemsize <= 12 else 8)
+
+
 @pytest.mark.parametrize("kt,vt", COMBOS)
 def test_edge_sizes_and_run_shapes(cuda, kt, vt):
-    # 2064, 4128, 12384: a last tile whose rows the tensor copies still cover
-    # (or, for 8-byte values, whose key rows they do not), next to the sizes
-    # whose ragged end is staged by plain loads
-    for i, n in enumerate([0, 1, 2, 3, 2064, 4095, 4096, 4097, 4128, 8192, 2 * 4096 + 1, 12384, 100003]):
+    # around one, two and three tiles T; T + 32 and 3T + 96: a last tile whose
+    # rows the tensor copies still cover, next to the sizes whose ragged end is
+    # staged by plain loads; 2064, 4128, 12384: ragged ends of other widths
+    t = _tile(kt, vt)
+    sizes = [0, 1, 2, 3, t // 2 + 16, t - 1, t, t + 1, t + 32, 2 * t, 2 * t + 1, 3 * t + 96,
+             2064, 4095, 4096, 4097, 4128, 8192, 12384, 100003]
+    for i, n in enumerate(sizes):
         for kind in ("geometric", "distinct", "one"):
             keys = _runs(kind, n, 5 + i).astype(NP[kt])
             vals = _vals(vt, n, 7 + i)
@@ -84,12 +92,16 @@ def test_zipf_runs_spanning_many_tiles(cuda, vt):
     _check(keys, vals, *_run(keys, vals))
 
 
-def test_runs_ending_on_tile_boundaries(cuda):
-    n = 4096 * 8
-    keys = (np.arange(n) // 4096).astype(np.int32)   # every run is exactly one tile
-    vals = np.ones(n, dtype=np.int32)
+@pytest.mark.parametrize("kt,vt", [("i32", "i32"), ("i32", "f64"), ("i64", "i64")])
+def test_runs_ending_on_tile_boundaries(cuda, kt, vt):
+    t = _tile(kt, vt)
+    n = t * 8
+    keys = (np.arange(n) // t).astype(NP[kt])   # every run is exactly one tile
+    vals = _vals(vt, n, 3)
     _check(keys, vals, *_run(keys, vals))
-    keys = (np.arange(n) // 4095).astype(np.int32)   # runs straddle every boundary
+    keys = (np.arange(n) // (t - 1)).astype(NP[kt])   # runs straddle every boundary
+    _check(keys, vals, *_run(keys, vals))
+    keys = (np.arange(n) // 16).astype(NP[kt])   # a run ends on every lane's last element
     _check(keys, vals, *_run(keys, vals))
 
 
