@@ -48,7 +48,7 @@ inline int max_ctas_per_sm(int op) {
   switch (op) {
     case kReduce: return 8;
     case kScan: return 2;
-    case kReduceByKey: return 2;
+    case kReduceByKey: return 3;  // the kernel caps it at 2 unless key and value are 4 bytes each
     case kMerge: return 3;
     default: return 1;
   }
@@ -57,7 +57,7 @@ inline Knobs default_knobs(int op) {
   switch (op) {
     case kReduce: return Knobs{4, 0};
     case kScan: return Knobs{2, 0};
-    case kReduceByKey: return Knobs{2, 0};
+    case kReduceByKey: return Knobs{3, 0};
     case kMerge: return Knobs{3, 0};
     default: return Knobs{1, 1};  // sort: L2 prefetch one residency ahead
   }

@@ -77,11 +77,14 @@ struct RbkCfg {
   static constexpr size_t KEY_BYTES = align_up(sizeof(K) * TILE, 1024);
   static constexpr size_t VAL_BYTES = align_up(sizeof(V) * TILE, 1024);
   static constexpr size_t BUF_BYTES = KEY_BYTES + VAL_BYTES;
+  // CTAs per SM: three when key and value are 4 bytes each (the kernel then
+  // fits in 64 registers a thread), else two
+  static constexpr int CTAS = sizeof(K) + sizeof(V) == 8 ? 3 : 2;
   // tile buffers in rotation: a tile holds one from its load, D iterations
-  // before its phase 1, to the end of its phase 1, so NB = D + 1; two CTAs per
-  // SM keep NB * BUF_BYTES under half the SM's shared memory
-  static constexpr int NB = BUF_BYTES <= 32 * 1024 ? 3 : 2;
-  static_assert(NB * BUF_BYTES <= 100 * 1024, "two CTAs per SM");
+  // before its phase 1, to the end of its phase 1, so NB = D + 1; as many as
+  // CTAS CTAs per SM leave room for
+  static constexpr int NB = CTAS == 3 ? 2 : (BUF_BYTES <= 32 * 1024 ? 3 : 2);
+  static_assert(CTAS * NB * BUF_BYTES <= 200 * 1024, "CTAS CTAs per SM");
   static constexpr int D = NB - 1;
   static constexpr size_t RUN_SLOT_BYTES = (sizeof(K) + sizeof(V)) * TILE;  // a tile's runs, at most TILE
   using P = Seg<V>;
@@ -96,7 +99,7 @@ size_t rbk_num_tiles(uint64_t n) {
 // kRbkRunSlots run slots per persistent CTA (a tile's runs wait there, keys
 // then values, from its phase 1 to its phase 2).
 constexpr int kRbkRunSlots = 4;
-constexpr size_t kRbkMaxGrid = 320;  // persistent CTAs at most (2 per SM)
+constexpr size_t kRbkMaxGrid = 480;  // persistent CTAs at most (3 per SM)
 template <typename K, typename V>
 size_t rbk_ring_offset(size_t tiles) {
   return align_up(kHeaderBytes + RbkCfg<K, V>::Status::bytes(tiles), 256);
@@ -452,7 +455,7 @@ __device__ __forceinline__ Seg<V> rbk_phase1_lane(unsigned char *buf, const K (*
 // failed.  Barrier phase parities are kept as bit masks (bit b: buffer b), so
 // no per-buffer array is indexed at run time.
 template <typename K, typename V, typename Src>
-__global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_constant__ Src src,
+__global__ void __launch_bounds__(kRbkThreads, RbkCfg<K, V>::CTAS) rbk_kernel(const __grid_constant__ Src src,
                                                              typename RbkCfg<K, V>::Status st, WsHeader *hdr,
                                                              unsigned char *ring, unsigned long long spin_limit_ns,
                                                              long long skip_publish_tile, unsigned int num_tiles) {
@@ -626,17 +629,19 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
   // ================= the compute warps =================
   const uint32_t e0 = (uint32_t)(warp * 32 + lane) * M;  // this lane's first element in every tile
   uint32_t fpar = 0u;  // bit b: parity of the next phase of s_full[b]
-  // the tiles of the last three iterations (index: iterations ago - 1), their
-  // run counts, whether they start with a head, and their head counts
+  // the tiles of the last three iterations (index: iterations ago - 1), each
+  // with its run count (bits 0-12), head count (bits 13-25) and whether it
+  // starts with a head (bit 26); counts are at most TILE <= 4096
+  static_assert(TILE <= 4096, "13-bit counts");
   unsigned int tq[3] = {NONE, NONE, NONE};
-  uint32_t rq[3] = {0u, 0u, 0u}, hq[3] = {0u, 0u, 0u}, cq[3] = {0u, 0u, 0u};
+  uint32_t iq[3] = {0u, 0u, 0u};
   bool ended = false;                 // an iteration has had no tile: no more loads
   bool bad = false;
 
   for (int it = 0;; ++it) {
     const int bt = it % NB, ps = it & 1;
     const unsigned int p = tq[2];  // phase 2 of t_{it-3}
-    const uint32_t pr = rq[2], ph = hq[2], pc = cq[2];
+    const uint32_t pr = iq[2] & 0x1fffu, pc = (iq[2] >> 13) & 0x1fffu, ph = iq[2] >> 26;
 
     // phase 2 of p reads its run slot (written before the last barrier):
     // start the loads of this thread's first two runs now, so that their L2
@@ -803,14 +808,10 @@ __global__ void __launch_bounds__(kRbkThreads, 2) rbk_kernel(const __grid_consta
 #pragma unroll
     for (int k = 2; k > 0; --k) {
       tq[k] = tq[k - 1];
-      rq[k] = rq[k - 1];
-      hq[k] = hq[k - 1];
-      cq[k] = cq[k - 1];
+      iq[k] = iq[k - 1];
     }
     tq[0] = t;
-    rq[0] = nruns;
-    hq[0] = h0;
-    cq[0] = aggc;
+    iq[0] = nruns | aggc << 13 | h0 << 26;
     if (t == NONE && tq[1] == NONE && tq[2] == NONE) break;
   }
 }
@@ -838,7 +839,7 @@ int rbk_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStrea
   host::KernelSetup ks;
   if ((st = host::kernel_setup<Site>(rbk_kernel<K, V, Src>, kRbkThreads, smem, &ks)) != BK_OK) return st;
   const tune::Knobs kn = tune::knobs_for(tune::kReduceByKey, (int)(sizeof(K) + sizeof(V)), (uint64_t)tiles * C::TILE);
-  const size_t per_sm = (size_t)std::min(std::max(kn.ctas_per_sm, 1), 2);
+  const size_t per_sm = (size_t)std::min(std::max(kn.ctas_per_sm, 1), C::CTAS);
   const unsigned grid = (unsigned)std::min<size_t>(tiles, std::min<size_t>((size_t)di.sm_count * per_sm, kRbkMaxGrid));
   unsigned char *ring = reinterpret_cast<unsigned char *>(d_ws) + rbk_ring_offset<K, V>(tiles);
   rbk_kernel<K, V, Src><<<grid, kRbkThreads, smem, stream>>>(src, status, hdr, ring, limit, dbg.skip_publish_tile,

@@ -30,16 +30,19 @@ if str(ROOT) not in sys.path:
 
 OPS = {"reduce": 0, "scan": 1, "reduce_by_key": 2, "merge": 3, "sort": 4}
 # the library's defaults (bk_tune.hpp default_knobs)
-DEFAULT = {"reduce": (4, 0), "scan": (2, 0), "reduce_by_key": (2, 0), "merge": (3, 0), "sort": (1, 1)}
+DEFAULT = {"reduce": (4, 0), "scan": (2, 0), "reduce_by_key": (3, 0), "merge": (3, 0), "sort": (1, 1)}
+# the kernel caps reduce_by_key at two CTAs per SM unless key and value are 4 bytes each
+DEFAULT_FOR = {("reduce_by_key", 12): (2, 0)}
 MARGIN = 0.03
 
 
-def choose(op, res):
+def choose(op, res, default=None):
     """The fastest shape if it beats the default by more than MARGIN, else the default."""
+    default = default or DEFAULT[op]
     best = min(res, key=lambda r: r[1])
-    dflt = [t for shape, t in res if shape == DEFAULT[op]]
+    dflt = [t for shape, t in res if shape == default]
     if dflt and best[1] > dflt[0] * (1.0 - MARGIN):
-        return DEFAULT[op]
+        return default
     return best[0]
 CLASS_N = [1 << 15, 1 << 19, 1 << 23, 1 << 26]
 # (op, label, element bytes, candidate (ctas_per_sm, prefetch) shapes)
@@ -48,7 +51,7 @@ PLAN = [
     ("reduce", "f64", 8, [(1, 0), (2, 0), (4, 0), (8, 0)]),
     ("scan", "f32", 4, [(1, 0), (2, 0)]),
     ("scan", "f64", 8, [(1, 0), (2, 0)]),
-    ("reduce_by_key", "i32/f32", 8, [(1, 0), (2, 0)]),
+    ("reduce_by_key", "i32/f32", 8, [(1, 0), (2, 0), (3, 0)]),
     ("reduce_by_key", "i32/f64", 12, [(1, 0), (2, 0)]),
     ("merge", "f32/u32", 8, [(1, 0), (2, 0), (3, 0)]),
     ("sort", "u32/u32", 8, [(1, 0), (1, 1), (1, 2)]),
@@ -136,7 +139,7 @@ def tune(quick=False):
                 _lib.check(lib.bk_tune_override(OPS[op], eb, sc, c, pf), "bk_tune_override")
                 res.append(((c, pf), _time(op, d, 5, inner)))
             _lib.check(lib.bk_tune_override(OPS[op], eb, sc, 0, 0), "bk_tune_override")
-            best = choose(op, res)
+            best = choose(op, res, DEFAULT_FOR.get((op, eb)))
             entries.append((OPS[op], eb, sc, best))
             record.append({"op": op, "dtype": label, "elem_bytes": eb, "size_class": sc, "n": n,
                            "candidates_ms": {f"ctas{c}_pf{pf}": t for (c, pf), t in res},
@@ -175,7 +178,7 @@ def from_json():
         for key, t in cell["candidates_ms"].items():
             c, pf = key.replace("ctas", "").split("_pf")
             res.append(((int(c), int(pf)), t))
-        best = choose(cell["op"], res)
+        best = choose(cell["op"], res, DEFAULT_FOR.get((cell["op"], cell["elem_bytes"])))
         cell["chosen"] = {"ctas_per_sm": best[0], "prefetch": best[1]}
         entries.append((OPS[cell["op"]], cell["elem_bytes"], cell["size_class"], best))
     prov["procedure"] = ("bulk_b200/tune.py: median of 5 timed calls (CUDA events) after 2 warm-up calls per "

@@ -15,7 +15,7 @@ from bulk_b200 import _lib
 ROOT = Path(__file__).resolve().parents[1]
 TABLE = ROOT / "bulk_b200" / "csrc" / "tuning_table.inc"
 OPS = {"kReduce": 0, "kScan": 1, "kReduceByKey": 2, "kMerge": 3, "kSort": 4}
-DEFAULTS = {0: (4, 0), 1: (2, 0), 2: (2, 0), 3: (3, 0), 4: (1, 1)}
+DEFAULTS = {0: (4, 0), 1: (2, 0), 2: (3, 0), 3: (3, 0), 4: (1, 1)}
 CLASS_N = [1, (1 << 16) - 1, 1 << 16, (1 << 20) - 1, 1 << 20, (1 << 24) - 1, 1 << 24, 1 << 30]
 CLASS_OF = [0, 0, 1, 1, 2, 2, 3, 3]
 
@@ -54,7 +54,8 @@ def test_override_wins_then_clears():
 
 
 @pytest.mark.parametrize("args", [(5, 4, 0, 1, 0), (-1, 4, 0, 1, 0), (0, 17, 0, 1, 0), (0, 4, 4, 1, 0),
-                                  (1, 4, 0, 3, 0), (3, 8, 0, 4, 0), (4, 8, 0, 2, 0), (0, 4, 0, 1, 5)])
+                                  (1, 4, 0, 3, 0), (2, 8, 0, 4, 0), (3, 8, 0, 4, 0), (4, 8, 0, 2, 0),
+                                  (0, 4, 0, 1, 5)])
 def test_override_bounds(args):
     assert bulk_b200.lib.bk_tune_override(*args) == _lib.BK_ERR_INVALID_ARGUMENT
 
