@@ -21,9 +21,10 @@ ops    = per-op GB/s: the headline's six calls, and the other benchmark
 serving = plain vs batched serving of a mixed request stream (the native loop
          bk_serve_run, driven by bulk_b200/serve.py: 40% sort_by_key u32/u32, 30% reduce_by_key i32/f32, 30% scan f32;
          sizes log-uniform in [2^10, 2^24], and a small-request variant in
-         [2^10, 2^16]): saturation req/s and, at 2000 req/s Poisson arrivals,
-         p50/p99 latency, for one call per request ("plain") and continuous
-         batching ("batched"); rank 0 only.
+         [2^10, 2^16]): saturation req/s and, at 2000 req/s Poisson arrivals
+         for 2 s, p50/p99 latency (over the latencies of 3 repeats with the
+         modes alternating), for one call per request ("plain") and
+         continuous batching ("batched"); rank 0 only.
 
 ``--impl reference`` times the reference's CPU implementation of the same
 reduce + scan on the host cores instead (rank 0 only).
@@ -592,8 +593,9 @@ def main(argv=None):
         }
     if rank == 0 and not args.no_serving:
         from bulk_b200 import serve
-        sv = serve.benchmark(saturation_requests=600, rate=2000.0, open_loop_s=1.0)
-        small = serve.benchmark(saturation_requests=2000, rate=2000.0, open_loop_s=1.0, hi=1 << 16)
+        sv = serve.benchmark(saturation_requests=600, rate=2000.0, open_loop_s=2.0, open_loop_repeats=3)
+        small = serve.benchmark(saturation_requests=2000, rate=2000.0, open_loop_s=2.0, open_loop_repeats=3,
+                                hi=1 << 16)
         line["serving"] = {"mix_2^10_2^24": sv, "mix_2^10_2^16": small}
         torch.cuda.empty_cache()
     if world > 1:

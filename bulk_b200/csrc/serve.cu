@@ -11,9 +11,11 @@
 // it, each with its own slice of the workspace) so that a round's sorts,
 // reduce_by_keys and scans run side by side on the device; a kind with a
 // single request in the round is issued as a plain single-array call, and a
-// round of at most two requests as plain calls on the caller's stream.  A
-// round's sorts run out of place: the batched sort reads each request's
-// source window and writes the request's own buffers.
+// round of at most four requests as plain calls on the caller's stream, at
+// once (not counted against max_inflight).  Batched mode's sorts run out of
+// place, lone ones of 2^20 elements and more too: the sort reads each
+// request's source window and writes the request's own buffers, where plain
+// mode copies the window into the buffers and sorts them in place.
 #include <algorithm>
 #include <chrono>
 #include <deque>
@@ -184,7 +186,12 @@ class Loop {
           waiting.push_back(r);
         }
       }
-      if (c_.mode == BK_SERVE_BATCHED && !waiting.empty() && (int)inflight.size() < c_.max_inflight) {
+      // a round small enough to go out as plain calls is issued at once, as
+      // plain mode would (queued behind the rounds in flight on the GPU,
+      // not held on the host until one of them completes); larger rounds
+      // wait for a free slot among the max_inflight
+      if (c_.mode == BK_SERVE_BATCHED && !waiting.empty() &&
+          ((int)inflight.size() < c_.max_inflight || waiting.size() <= (size_t)kPlainRound)) {
         const double ti = now();
         for (Req *r : waiting) r->rec->start_s = ti;
         if ((st = issue_batches(waiting)) != BK_OK) return finish(st, stats, t0);
@@ -298,7 +305,23 @@ class Loop {
     }
   }
 
-  static constexpr int kPlainRound = 2;
+  // Batched mode, a request issued alone: as its plain call, except that a
+  // sort of at least kLoneDirect elements reads its source window directly (a
+  // one-item out-of-place batch) instead of first copying the window into its
+  // buffers.  Below that the batch call's larger launches cost more than the
+  // copy saves (measured on a B200: open-loop p99 of the 2^10-2^16 mix 5 %
+  // higher with every lone sort out of place, of the 2^10-2^24 mix 8 % lower).
+  static constexpr uint64_t kLoneDirect = 1ull << 20;
+  int issue_lone(Req *q, cudaStream_t s, void *ws, size_t ws_bytes) {
+    if (q->r->kind != BK_SERVE_SORT || q->r->n < kLoneDirect) return issue_one_on(q, s, ws, ws_bytes);
+    ++calls_;
+    const uint64_t o = q->r->src_offset;
+    const bk_sort_copy_item_u32_u32 it{c_.sort_keys + o, c_.sort_vals + o, buf<uint32_t>(q, 0), buf<uint32_t>(q, 1),
+                                       q->r->n};
+    return bk_sort_by_key_u32_u32_copy_batch(&it, 1u, ws, ws_bytes, (bk_stream_t)s);
+  }
+
+  static constexpr int kPlainRound = 4;
 
   // One admission round: per kind, one batched call (at most BK_BATCH_MAX
   // arrays each; sorts out of place, from the requests' source windows), or
@@ -308,13 +331,13 @@ class Loop {
   // caller's stream (its slice is free there: the caller's stream has
   // joined every earlier use of it).
   int issue_batches(const std::vector<Req *> &reqs) {
-    // a round of one or two requests (light load) is issued as plain calls on
+    // a round of up to four requests (light load) is issued as plain calls on
     // the caller's stream: batch descriptors and stream fork/join would only
     // add latency there
     if (reqs.size() <= (size_t)kPlainRound) {
       for (Req *r : reqs) {
         const int kind = (int)r->r->kind;
-        const int st = issue_one_on(r, st_, ws_[kind], ws_bytes_[kind]);
+        const int st = issue_lone(r, st_, ws_[kind], ws_bytes_[kind]);
         if (st != BK_OK) return st;
       }
       return BK_OK;
@@ -332,7 +355,7 @@ class Loop {
         s = ks_[kind];
         if ((st = host::from_cuda(cudaStreamWaitEvent(s, fork, 0))) != BK_OK) return st;
       }
-      if (by[kind].size() == 1) st = issue_one_on(by[kind][0], s, ws_[kind], ws_bytes_[kind]);
+      if (by[kind].size() == 1) st = issue_lone(by[kind][0], s, ws_[kind], ws_bytes_[kind]);
       else st = issue_kind(kind, by[kind], s);
       if (st != BK_OK) return st;
       if (kinds > 1) {

@@ -16,10 +16,12 @@ pre-generated source array of its kind, so it depends only on the id.
 
 The loop itself is native (``bk_serve_run`` in libbulkb200.so): admission in
 arrival order against an HBM budget, a pooled first-fit allocator over one
-device buffer, issue on one stream, completion by event polling.  ``plain``
-issues every admitted request as its own call (the single-array entry
-points); ``batched`` issues every admitted request that has arrived at once,
-one batched call per kind, with at most ``max_inflight`` batches queued.
+device buffer, issue on the caller's stream, completion by event polling.
+``plain`` issues every admitted request as its own call (the single-array
+entry points); ``batched`` issues every admitted request that has arrived at
+once as one round, one batched call per kind (the kinds side by side on
+streams of their own), with at most ``max_inflight`` rounds of more than four
+requests queued (smaller rounds go out at once as plain calls).
 Latency = completion time - arrival time, on the host's steady clock.  This
 module builds the request stream and the sources, and reads the records.
 """
@@ -209,7 +211,7 @@ class Server:
             if self.keep:
                 self.results[r.rid] = self._result(r, recs[i].out)
         lat = np.array([r.done - r.arrival for r in pending]) if count else np.zeros(1)
-        return {"mode": mode, "requests": count, "makespan_s": stats.makespan_s,
+        return {"mode": mode, "requests": count, "makespan_s": stats.makespan_s, "latency_s": lat,
                 "req_per_s": count / stats.makespan_s if stats.makespan_s > 0 else math.inf,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "pool_high_water_bytes": stats.pool_high_water, "calls": stats.calls, "batches": stats.batches}
@@ -224,30 +226,48 @@ class Server:
         return (v(out[0], r.n, torch.float32).clone(),)
 
 
-def benchmark(saturation_requests: int = 600, rate: float = 2000.0, open_loop_s: float = 1.0, seed: int = 1000,
-              lo: int = 1 << 10, hi: int = 1 << 24, budget_bytes: int = 32 << 30, device="cuda") -> dict:
+def benchmark(saturation_requests: int = 600, rate: float = 2000.0, open_loop_s: float = 2.0, seed: int = 1000,
+              lo: int = 1 << 10, hi: int = 1 << 24, budget_bytes: int = 32 << 30, device="cuda",
+              open_loop_repeats: int = 3) -> dict:
     """Plain vs batched serving of the mixed request stream.
 
     saturation: `saturation_requests` requests all arriving at t = 0 (req/s is
     the throughput); open loop: Poisson arrivals at `rate` for `open_loop_s`
-    seconds (latency percentiles at that load).  Both modes serve the same
-    requests, after one warm-up run each."""
+    seconds (latency percentiles at that load), `open_loop_repeats` times with
+    the two modes alternating, each repeat on its own arrival sequence; the
+    reported percentiles are over the latencies of all repeats together (the
+    p99 of one short run is one of its few largest latencies, which moves by
+    several percent from run to run).  Both modes serve the same requests,
+    after one warm-up run each."""
     src = Sources(hi, device=device)
     pool = DevicePool(min(budget_bytes, 24 << 30) + (1 << 24), device=device)
     out = {"config": {"mix": "40% sort_by_key u32/u32, 30% reduce_by_key i32/f32 (runs mean 32), 30% scan f32",
                       "sizes": f"log-uniform [{lo}, {hi}]", "rate_req_s": rate, "budget_bytes": budget_bytes,
-                      "saturation_requests": saturation_requests, "open_loop_s": open_loop_s}}
-    for mode in ("plain", "batched"):
-        server = Server(src, pool, budget_bytes)
+                      "saturation_requests": saturation_requests, "open_loop_s": open_loop_s,
+                      "open_loop_repeats": open_loop_repeats}}
+    modes = ("plain", "batched")
+    servers = {mode: Server(src, pool, budget_bytes) for mode in modes}
+    for mode in modes:
+        server = servers[mode]
         server.run(make_requests(64, math.inf, seed + 1, lo, hi), mode)  # warm-up (workspaces, kernels)
         torch.cuda.synchronize()
         sat = server.run(make_requests(saturation_requests, math.inf, seed, lo, hi), mode)
         torch.cuda.synchronize()
-        ol = server.run(make_requests(max(1, int(rate * open_loop_s)), rate, seed + 2, lo, hi), mode)
-        torch.cuda.synchronize()
         out[mode] = {"saturation_req_s": sat["req_per_s"], "saturation_p99_ms": sat["p99_ms"],
-                     "open_loop_p50_ms": ol["p50_ms"], "open_loop_p99_ms": ol["p99_ms"],
-                     "open_loop_req_s": ol["req_per_s"], "saturation_calls": sat["calls"],
-                     "saturation_batches": sat["batches"]}
+                     "saturation_calls": sat["calls"], "saturation_batches": sat["batches"]}
+    runs = {mode: [] for mode in modes}
+    for r in range(max(1, open_loop_repeats)):
+        reqs = max(1, int(rate * open_loop_s))
+        for mode in modes:
+            runs[mode].append(servers[mode].run(make_requests(reqs, rate, seed + 2 + r, lo, hi), mode))
+            torch.cuda.synchronize()
+    for mode in modes:
+        lat = np.concatenate([o["latency_s"] for o in runs[mode]])
+        out[mode].update({
+            "open_loop_p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "open_loop_p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "open_loop_req_s": float(np.median([o["req_per_s"] for o in runs[mode]])),
+            "open_loop_requests": int(lat.size),
+            "open_loop_p99_runs_ms": [o["p99_ms"] for o in runs[mode]]})
     out["batched_over_plain_req_s"] = out["batched"]["saturation_req_s"] / out["plain"]["saturation_req_s"]
     return out

@@ -362,12 +362,17 @@ BK_API int bk_sort_by_key_f64_u64_copy_batch(const bk_sort_copy_item_f64_u64 *it
 
 /* ---- serving loop -----------------------------------------------------------
  * No counterpart in the reference, whose drivers run one array at a time.
- * bk_serve_run answers a stream of mixed requests on one stream, either one
- * library call per request (BK_SERVE_PLAIN: the single-array entry points
- * above, sort inputs copied with cudaMemcpyAsync) or by continuous batching
- * (BK_SERVE_BATCHED: every admitted request that has arrived is issued at
- * once, one *_batch call per kind, sort inputs gathered by one copy kernel;
- * at most max_inflight batches are queued on the stream).  A request reads
+ * bk_serve_run answers a stream of mixed requests on the caller's stream,
+ * either one library call per request (BK_SERVE_PLAIN: the single-array entry
+ * points above, sort inputs copied with cudaMemcpyAsync) or by continuous
+ * batching (BK_SERVE_BATCHED: every admitted request that has arrived is
+ * issued at once as one round -- per kind one *_batch call, sorts out of
+ * place from the requests' source windows, the kinds on streams of their
+ * own forked from the caller's stream and joined back to it; a kind with one
+ * request, and a round of at most four requests, go out as plain calls (a
+ * sort of 2^20 elements or more as a one-item out-of-place batch); at most
+ * max_inflight rounds of more than four requests are queued at once).
+ * A request reads
  * a window of the caller's source arrays; its own buffers (sort: keys and
  * payload, sorted in place; rbk: out_keys, out_vals, count; scan: output)
  * come from a first-fit pool over the caller's device buffer, and requests
@@ -412,7 +417,7 @@ typedef struct bk_serve_config {
   uint64_t budget_bytes;
   bk_stream_t stream;
   int32_t mode;              /* BK_SERVE_PLAIN / BK_SERVE_BATCHED */
-  int32_t max_inflight;      /* batched: batches queued on the stream at once (>= 1) */
+  int32_t max_inflight;      /* batched: rounds of more than four requests queued at once (>= 1) */
   int32_t keep_buffers;      /* 1: buffers are not reused, so every result stays readable */
   int32_t reserved;
   double timeout_s;
