@@ -166,6 +166,37 @@ def test_serving_results_match_each_request_alone(cuda, mode):
 
 
 @pytest.mark.gpu
+def test_batched_small_rounds_match_each_request_alone(cuda):
+    """Spaced arrivals: batched mode issues rounds of up to four requests as
+    plain calls, and a lone sort of 2^20 elements or more as a one-item
+    out-of-place batch reading its source window; every result must still be
+    the request's own."""
+    src = serve.Sources(1 << 21)
+    pool = serve.DevicePool(1 << 28)
+    server = serve.Server(src, pool, budget_bytes=1 << 27, keep_results=True)
+    reqs = serve.make_requests(24, 400.0, seed=31, lo=1 << 20, hi=1 << 21)
+    assert any(r.kind == "sort" for r in reqs)
+    stats = server.run(reqs, "batched")
+    assert stats["requests"] == 24
+    torch.cuda.synchronize()
+    for r in reqs:
+        got = server.results[r.rid]
+        want = _alone(server, r)
+        if r.kind == "sort":
+            assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), r
+        elif r.kind == "rbk":
+            c = int(want[2].item())
+            assert int(got[2].item()) == c and torch.equal(got[0][:c], want[0][:c]), r
+            o = src.offset(r)
+            vals = src.rbk_vals[o:o + r.n]
+            assert torch.all((got[1][:c].double() - want[1][:c].double()).abs() <= _bound(vals)[-1] + 1e-30), r
+        else:
+            o = src.offset(r)
+            x = src.scan_vals[o:o + r.n]
+            assert torch.all((got[0].double() - want[0].double()).abs() <= _bound(x)), r
+
+
+@pytest.mark.gpu
 def test_admission_respects_the_budget(cuda):
     src = serve.Sources(1 << 18)
     pool = serve.DevicePool(1 << 26)
