@@ -161,17 +161,29 @@ def reduce(x: torch.Tensor, init=0, op: str = "sum", out: torch.Tensor | None = 
 
 def inclusive_scan(x: torch.Tensor, init=0, op: str = "sum", out: torch.Tensor | None = None,
                    stream: torch.cuda.Stream | None = None) -> torch.Tensor:
-    """out[i] = init (+) x[0] (+) ... (+) x[i]; ``out`` may be ``x`` (in place)."""
+    """out[i] = init (+) x[0] (+) ... (+) x[i]; ``out`` may be ``x`` (in place).
+
+    ``init`` may be a device tensor of x's dtype (one element, or a view of
+    one, e.g. the last output of a previous scan): it is then read on the
+    device when the scan runs, with no copy to the host."""
     dev = _require_cuda(x, out)
     tag = dtype_tag(x.dtype)
     if out is None:
         out = torch.empty_like(x)
+    dinit = isinstance(init, torch.Tensor)
+    if dinit:
+        if not init.is_cuda or init.device != dev or init.dtype != x.dtype or init.numel() != 1:
+            raise ValueError("a tensor init must be one element of x's dtype on x's device")
     with torch.cuda.device(dev):
         so = _stream_obj(stream, dev)
         s = so.cuda_stream
         ws, wsb = _ws("inclusive_scan", tag, None, x.numel(), dev, so)
-        fn = getattr(lib, f"bk_inclusive_scan_{op}_{tag}")
-        check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
+        if dinit:
+            fn = getattr(lib, f"bk_inclusive_scan_{op}_{tag}_dinit")
+            check(fn(_ptr(x), x.numel(), _ptr(init), _ptr(out), ws, wsb, s), fn.__name__)
+        else:
+            fn = getattr(lib, f"bk_inclusive_scan_{op}_{tag}")
+            check(fn(_ptr(x), x.numel(), init, _ptr(out), ws, wsb, s), fn.__name__)
     return out
 
 

@@ -93,14 +93,18 @@ struct ScanOne {
   T *out;
   uint64_t n;
   T init;
-  int tma;           // in and out 16-byte aligned
-  uint64_t covered;  // kSwz: leading elements inside whole rows of both views
+  const T *init_ptr;  // init read from device memory instead (the _dinit entry points), else null
+  int tma;            // in and out 16-byte aligned
+  uint64_t covered;   // kSwz: leading elements inside whole rows of both views
   __device__ __forceinline__ ScanTile<T> tile(unsigned int t) const {
     const uint64_t base = (uint64_t)t * ScanCfg<T>::TILE;
     const uint64_t rem = n - base;
     const uint32_t cnt = (uint32_t)(rem < (uint64_t)ScanCfg<T>::TILE ? rem : (uint64_t)ScanCfg<T>::TILE);
     const bool t_tma = kSwz ? (base + cnt <= covered) : (tma != 0);
-    return ScanTile<T>{in + base, out + base, cnt, t == 0u, t_tma, init, t};
+    // only the first tile uses init; a device-resident one was written before
+    // this launch (stream order) and is read-only during it
+    const T iv = (t == 0u && init_ptr != nullptr) ? __ldg(init_ptr) : init;
+    return ScanTile<T>{in + base, out + base, cnt, t == 0u, t_tma, iv, t};
   }
   __device__ __forceinline__ const CUtensorMap *in_map() const { return &imap; }
   __device__ __forceinline__ const CUtensorMap *out_map() const { return &omap; }
@@ -653,8 +657,12 @@ int scan_run(const Src &src, size_t tiles, void *d_ws, size_t ws_bytes, cudaStre
   return host::launch_status();
 }
 
+// init_ptr: when not null, init is read from device memory at run time (so a
+// scan can continue from a value still on the device: the last output of the
+// previous chunk of a stream, say) and `init` is ignored.
 template <typename T, typename Op>
-int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t ws_bytes, cudaStream_t stream) {
+int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t ws_bytes, cudaStream_t stream,
+                const T *init_ptr = nullptr) {
   if (n == 0) {
     host::DeviceInfo di;
     return host::device_info(&di);
@@ -668,6 +676,8 @@ int scan_launch(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, size_t 
   src.out = d_out;
   src.n = n;
   src.init = init;
+  src.init_ptr = init_ptr;
+  if (init_ptr != nullptr && !host::aligned_to<T>(init_ptr)) return BK_ERR_MISALIGNED;
   src.tma = tma;
   if constexpr (ScanOne<T>::kSwz) {
     // row views of the input and output: the tiles inside whole 128-byte rows
@@ -751,6 +761,13 @@ size_t scan_workspace_bytes(int dtype, uint64_t n) {
   extern "C" int bk_inclusive_scan_##OPNAME##_##TN(const T *d_in, uint64_t n, T init, T *d_out, void *d_ws, \
                                                    size_t ws_bytes, bk_stream_t stream) {                   \
     return bk::scan_launch<T, bk::OPT<T>>(d_in, n, init, d_out, d_ws, ws_bytes, (cudaStream_t)stream);      \
+  }                                                                                                          \
+  extern "C" int bk_inclusive_scan_##OPNAME##_##TN##_dinit(const T *d_in, uint64_t n, const T *d_init,       \
+                                                           T *d_out, void *d_ws, size_t ws_bytes,            \
+                                                           bk_stream_t stream) {                             \
+    if (d_init == nullptr) return BK_ERR_INVALID_ARGUMENT;                                                   \
+    return bk::scan_launch<T, bk::OPT<T>>(d_in, n, bk::OPT<T>::identity(), d_out, d_ws, ws_bytes,            \
+                                          (cudaStream_t)stream, d_init);                                     \
   }
 
 #define BK_DEFINE_SCAN_ALL_T(OPNAME, OPT)      \

@@ -161,6 +161,30 @@ BK_API int bk_inclusive_scan_max_u64(const uint64_t *d_in, uint64_t n, uint64_t 
 BK_API int bk_inclusive_scan_max_f32(const float *d_in, uint64_t n, float init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_inclusive_scan_max_f64(const double *d_in, uint64_t n, double init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 
+/* The same with init read from device memory when the scan runs: *d_init
+ * (non-null, aligned) replaces init, so a scan can continue from a value that
+ * is still on the device -- e.g. the last output of the previous chunk of a
+ * stream (d_init = d_out_prev + n_prev - 1), with no copy to the host between
+ * the chunks.  The reference's scan takes init by value (scan.cu:87). */
+BK_API int bk_inclusive_scan_sum_i32_dinit(const int32_t *d_in, uint64_t n, const int32_t *d_init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_u32_dinit(const uint32_t *d_in, uint64_t n, const uint32_t *d_init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_i64_dinit(const int64_t *d_in, uint64_t n, const int64_t *d_init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_u64_dinit(const uint64_t *d_in, uint64_t n, const uint64_t *d_init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_f32_dinit(const float *d_in, uint64_t n, const float *d_init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_sum_f64_dinit(const double *d_in, uint64_t n, const double *d_init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_i32_dinit(const int32_t *d_in, uint64_t n, const int32_t *d_init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_u32_dinit(const uint32_t *d_in, uint64_t n, const uint32_t *d_init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_i64_dinit(const int64_t *d_in, uint64_t n, const int64_t *d_init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_u64_dinit(const uint64_t *d_in, uint64_t n, const uint64_t *d_init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_f32_dinit(const float *d_in, uint64_t n, const float *d_init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_min_f64_dinit(const double *d_in, uint64_t n, const double *d_init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_i32_dinit(const int32_t *d_in, uint64_t n, const int32_t *d_init, int32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_u32_dinit(const uint32_t *d_in, uint64_t n, const uint32_t *d_init, uint32_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_i64_dinit(const int64_t *d_in, uint64_t n, const int64_t *d_init, int64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_u64_dinit(const uint64_t *d_in, uint64_t n, const uint64_t *d_init, uint64_t *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_f32_dinit(const float *d_in, uint64_t n, const float *d_init, float *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+BK_API int bk_inclusive_scan_max_f64_dinit(const double *d_in, uint64_t n, const double *d_init, double *d_out, void *d_ws, size_t ws_bytes, bk_stream_t stream);
+
 
 /* ---- merge ----------------------------------------------------------------
  * Stable merge of two sorted ranges under operator<: equal keys keep A before

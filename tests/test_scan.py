@@ -66,6 +66,42 @@ def test_misaligned_pointers(cuda, tag):
     _check(tag, "sum", x[1:], 0, host(out))
 
 
+@pytest.mark.parametrize("tag", ["i32", "f32", "f64"])
+def test_device_init_matches_host_init(cuda, tag):
+    # init read on the device (the _dinit entry points) gives the same bits
+    # as the same init passed by value: it enters the same fold
+    for i, n in enumerate([1, 777, 8192 * 3 + 5, 1000003]):
+        x = gen(tag, n, 300 + i)
+        init = NP[tag](7 if tag == "i32" else -1.25)
+        d = dev(x)
+        want = bulk_b200.inclusive_scan(d, init)
+        got = bulk_b200.inclusive_scan(d, torch.tensor([init], device=cuda))
+        assert torch.equal(got, want), (tag, n)
+
+
+def test_chained_chunks_equal_one_scan(cuda):
+    # a stream scanned chunk by chunk, each chunk starting from the previous
+    # chunk's last output still on the device, equals one scan of the whole
+    x = gen("i32", 3_000_001, 9)
+    d = dev(x)
+    out = torch.empty_like(d)
+    bounds = [0, 1, 4097, 1_000_000, 1_000_003, 2_500_000, 3_000_001]
+    for lo, hi in zip(bounds, bounds[1:]):
+        init = 13 if lo == 0 else out[lo - 1:lo]
+        bulk_b200.inclusive_scan(d[lo:hi], init, out=out[lo:hi])
+    _check("i32", "sum", x, 13, host(out))
+
+
+def test_device_init_rejects_a_null_pointer(cuda):
+    d = torch.ones(100, dtype=torch.int32, device=cuda)
+    ws = torch.zeros(bulk_b200.workspace_bytes("inclusive_scan", "i32", None, 100), dtype=torch.uint8, device=cuda)
+    st = bulk_b200.lib.bk_inclusive_scan_sum_i32_dinit(d.data_ptr(), 100, None, d.data_ptr(), ws.data_ptr(),
+                                                       ws.numel(), torch.cuda.current_stream().cuda_stream)
+    assert st == _lib.BK_ERR_INVALID_ARGUMENT
+    with pytest.raises(ValueError):
+        bulk_b200.inclusive_scan(d, torch.tensor([1.0], device=cuda))  # wrong dtype
+
+
 def test_repeated_calls_reuse_the_workspace(cuda):
     x = gen("f32", (1 << 22) + 7, 8)
     d = dev(x)
