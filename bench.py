@@ -11,8 +11,9 @@ value  = algorithmic bytes per step (reduce N*s, scan 2*N*s) / device time,
          GPU: replicas, weak scaling).
 e2e    = the same through the C-ABI with host buffers: pinned-host -> device
          copies of the step's inputs and device -> host copies of every result
-         inside the timed region (one stream per array, so copies in the two
-         directions overlap).
+         inside the timed region (in chunks of 2^25 elements on two streams,
+         each chunk's scan starting from the previous chunk's last output on
+         the device, so copies in the two directions overlap).
 ops    = per-op GB/s: the headline's six calls, and the other benchmark
          configurations (merge_by_key 2 x 2^26 f32/u32, stable sort_by_key
          2^26 u32/u64 keys with u32 payload, reduce_by_key 2^27 i32 keys with
@@ -319,17 +320,24 @@ def headline(args, device, rank, world):
     return ms, per, clk.summary(), xs
 
 
+E2E_CHUNK = 1 << 25  # elements per copy chunk of the end-to-end leg
+
+
 def e2e(args, device, xs):
     """Same workload through the public API with host buffers (pinned), copies timed.
 
-    Each dtype's array goes through its own stream (copy in, reduce, scan,
-    copy out), so one array's copy to the host overlaps the next one's copy to
-    the device: the two directions use separate copy engines."""
+    A two-stream pipeline over chunks of E2E_CHUNK elements: one stream copies
+    every array to the device chunk by chunk; the other waits for each chunk,
+    scans it starting from the previous chunk's last output (read on the
+    device: inclusive_scan with a device-tensor init), copies the chunk's
+    output back, and reduces each array once its last chunk is in.  So copies
+    to the device and copies back (separate copy engines) overlap for the
+    whole step, not just between arrays."""
     import torch
 
     import bulk_b200
     stream = torch.cuda.current_stream(device)
-    streams = {k: torch.cuda.Stream(device) for k, _ in DTYPES}
+    up, down = torch.cuda.Stream(device), torch.cuda.Stream(device)
     h_in = {k: v.cpu().pin_memory() for k, v in xs.items()}
     h_scan = {k: torch.empty_like(v, device="cpu").pin_memory() for k, v in xs.items()}
     h_red = {k: torch.empty(1, dtype=v.dtype).pin_memory() for k, v in xs.items()}
@@ -338,16 +346,26 @@ def e2e(args, device, xs):
     d_red = {k: torch.empty(1, dtype=v.dtype, device=device) for k, v in xs.items()}
     h2d = sum(v.numel() * v.element_size() for v in h_in.values())
     d2h = sum(v.numel() * v.element_size() for v in h_scan.values()) + sum(v.element_size() for v in h_red.values())
+    chunks = [(k, lo, min(xs[k].numel(), lo + E2E_CHUNK)) for k, _ in DTYPES
+              for lo in range(0, xs[k].numel(), E2E_CHUNK)]
+    arrived = [torch.cuda.Event() for _ in chunks]
 
     def step():
-        for k, _ in DTYPES:
-            s = streams[k]
-            with torch.cuda.stream(s):
-                d_in[k].copy_(h_in[k], non_blocking=True)
-                bulk_b200.reduce(d_in[k], 0, out=d_red[k], stream=s)
-                bulk_b200.inclusive_scan(d_in[k], 0, out=d_out[k], stream=s)
-                h_red[k].copy_(d_red[k], non_blocking=True)
-                h_scan[k].copy_(d_out[k], non_blocking=True)
+        # this step's copies overwrite the inputs the previous step's scans read
+        up.wait_stream(down)
+        with torch.cuda.stream(up):
+            for (k, lo, hi), ev in zip(chunks, arrived):
+                d_in[k][lo:hi].copy_(h_in[k][lo:hi], non_blocking=True)
+                ev.record(up)
+        with torch.cuda.stream(down):
+            for (k, lo, hi), ev in zip(chunks, arrived):
+                down.wait_event(ev)
+                init = 0 if lo == 0 else d_out[k][lo - 1:lo]
+                bulk_b200.inclusive_scan(d_in[k][lo:hi], init, out=d_out[k][lo:hi], stream=down)
+                h_scan[k][lo:hi].copy_(d_out[k][lo:hi], non_blocking=True)
+                if hi == xs[k].numel():
+                    bulk_b200.reduce(d_in[k], 0, out=d_red[k], stream=down)
+                    h_red[k].copy_(d_red[k], non_blocking=True)
 
     steps = max(1, min(args.steps, args.e2e_steps))
     for _ in range(min(args.warmup, 3)):
@@ -355,12 +373,12 @@ def e2e(args, device, xs):
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    for s in streams.values():
-        s.wait_event(a)
+    up.wait_event(a)
+    down.wait_event(a)
     for _ in range(steps):
         step()
-    for s in streams.values():
-        stream.wait_stream(s)
+    stream.wait_stream(up)
+    stream.wait_stream(down)
     b.record(stream)
     torch.cuda.synchronize()
     return a.elapsed_time(b) / steps, h2d, d2h, steps

@@ -68,15 +68,18 @@ def test_misaligned_pointers(cuda, tag):
 
 @pytest.mark.parametrize("tag", ["i32", "f32", "f64"])
 def test_device_init_matches_host_init(cuda, tag):
-    # init read on the device (the _dinit entry points) gives the same bits
-    # as the same init passed by value: it enters the same fold
+    # init read on the device (the _dinit entry points) enters the same fold
+    # as init passed by value: integers give the same bits; float prefixes
+    # stay within the oracle's bound (float scans over several tiles are not
+    # bitwise reproducible run to run: the look-back's decomposition varies)
     for i, n in enumerate([1, 777, 8192 * 3 + 5, 1000003]):
         x = gen(tag, n, 300 + i)
         init = NP[tag](7 if tag == "i32" else -1.25)
         d = dev(x)
-        want = bulk_b200.inclusive_scan(d, init)
         got = bulk_b200.inclusive_scan(d, torch.tensor([init], device=cuda))
-        assert torch.equal(got, want), (tag, n)
+        if tag == "i32":
+            assert torch.equal(got, bulk_b200.inclusive_scan(d, init)), (tag, n)
+        _check(tag, "sum", x, init, host(got))
 
 
 def test_chained_chunks_equal_one_scan(cuda):
