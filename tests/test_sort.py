@@ -124,6 +124,31 @@ def test_signed_zeros_infinities_and_denormals_keep_stable_order(cuda, tag):
         assert np.array_equal(host(gv), wv), n
 
 
+@pytest.mark.parametrize("tag", ["u32", "i64"])
+def test_views_off_16_byte_boundaries(cuda, tag):
+    """Keys and payloads starting 1-3 elements past a 16-byte boundary: the
+    scatter reads such tiles directly instead of by bulk copy.  In place and
+    out of place (the batch entry point with separate sources), against the
+    oracle."""
+    from bulk_b200 import batch
+    n = 3 * 4096 + 1234
+    for off in (1, 2, 3):
+        keys = _keys(tag, n, 40 + off, coarse=(off == 2))
+        vals = np.arange(n, dtype=np.uint32)
+        wk, wv = oracle.stable_sort_by_key(keys, vals)
+        kb = torch.zeros(n + off, dtype=dev(keys).dtype, device=cuda)
+        vb = torch.zeros(n + off, dtype=torch.int32, device=cuda)
+        kb[off:].copy_(dev(keys))
+        vb[off:].copy_(dev(vals.view(np.int32)))
+        gk, gv = bulk_b200.stable_sort_by_key(kb[off:], vb[off:])
+        assert np.array_equal(host(gk), wk) and np.array_equal(host(gv).view(np.uint32), wv), (tag, off)
+        kb[off:].copy_(dev(keys))
+        vb[off:].copy_(dev(vals.view(np.int32)))
+        ok, ov = torch.empty(n + 1, dtype=kb.dtype, device=cuda), torch.empty(n + 1, dtype=torch.int32, device=cuda)
+        (gk,), (gv,) = batch.stable_sort_by_key_copy_batch([kb[off:]], [vb[off:]], [ok[1:]], [ov[1:]])
+        assert np.array_equal(host(gk), wk) and np.array_equal(host(gv).view(np.uint32), wv), (tag, off, "copy")
+
+
 @pytest.mark.slow
 def test_merge_path_at_2_30(cuda):
     """2^30 elements, the first size sorted by merging: i32 keys with many
