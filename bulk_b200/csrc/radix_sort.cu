@@ -187,11 +187,11 @@ __device__ __forceinline__ void rs_prefetch_tile(const Src &src, unsigned int g,
 }
 
 // Six CTAs per SM (40 registers) for 4-byte keys on one array: the u32/u32
-// sort at 2^26 ran 1.1 % faster than with the compiler's 48 registers (five
-// CTAs) on a B200; 8-byte keys and a batch's tile lookup would spill there.
+// sort at 2^26 ran 1.1 % faster than with five (48 registers) on a B200;
+// 8-byte keys and a batch's tile lookup would spill there and keep five.
 template <typename K, typename P, typename Src>
 constexpr int rs_up_min_blocks() {
-  return sizeof(K) == 4 && std::is_same<Src, RsOne<K, P>>::value ? 6 : 1;
+  return sizeof(K) == 4 && std::is_same<Src, RsOne<K, P>>::value ? 6 : 5;
 }
 template <typename K, typename P, typename Src>
 __global__ void __launch_bounds__(kRsThreads, rs_up_min_blocks<K, P, Src>()) rs_upsweep_kernel(const __grid_constant__ Src src, int pass,
@@ -382,6 +382,7 @@ __global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downswe
 // replace the three launches a pass of the global-memory path takes, and
 // global memory is read once and written once.
 constexpr int kRsClusterMax = 16;  // CTAs (non-portable above 8)
+constexpr int kRsClThreads = 1024;  // four items a thread: short ranking chains, 32 warps an SM
 
 __device__ __forceinline__ uint32_t rs_cluster_rank() {
   uint32_t r;
@@ -428,22 +429,22 @@ constexpr size_t rs_cluster_smem_bytes() {
 }
 
 template <typename K, typename P>
-__global__ void __launch_bounds__(kRsThreads, 1) rs_cluster_kernel(K *keys, P *vals, uint32_t n) {
-  constexpr int ITEMS = kRsItems;
+__global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P *vals, uint32_t n) {
+  constexpr int ITEMS = kRsTile / kRsClThreads, WARPS = kRsClThreads / 32;
   constexpr size_t BB = rs_cluster_buf_bytes<K, P>();
   constexpr size_t VOFF = align_up(sizeof(K) * kRsTile, 16);
   extern __shared__ __align__(16) unsigned char rs_cl_smem[];
-  __shared__ unsigned int s_whist[kRsWarps][kRsBins];  // per-warp digit counters, then staging starts
+  __shared__ unsigned int s_whist[WARPS][kRsBins];  // per-warp digit counters, then staging starts
   __shared__ unsigned int s_cnt[kRsBins];              // this tile's count of each digit (read by the peers)
   __shared__ unsigned int s_dst[kRsBins];  // output position of staged position 0 for digit d
-  __shared__ unsigned int s_scan[kRsWarps + 1];
+  __shared__ unsigned int s_scan[WARPS + 1];
   auto bk_ = [&](int b) { return reinterpret_cast<K *>(rs_cl_smem + b * BB); };
   auto bv_ = [&](int b) { return reinterpret_cast<P *>(rs_cl_smem + b * BB + VOFF); };
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t me = rs_cluster_rank(), csize = rs_cluster_size();
   const uint32_t base = me * (uint32_t)kRsTile;
   const int count = (int)((n - base) < (uint32_t)kRsTile ? (n - base) : (uint32_t)kRsTile);
-  for (int i = tid; i < count; i += kRsThreads) {
+  for (int i = tid; i < count; i += kRsClThreads) {
     bk_(0)[i] = keys[base + i];
     if constexpr (has_payload<P>()) bv_(0)[i] = vals[base + i];
   }
@@ -451,7 +452,7 @@ __global__ void __launch_bounds__(kRsThreads, 1) rs_cluster_kernel(K *keys, P *v
   for (int pass = 0; pass < rs_passes<K>(); ++pass) {
     const int in = pass & 1, out = in ^ 1;
     const int shift = 8 * pass;
-    for (int i = tid; i < kRsWarps * kRsBins; i += kRsThreads) (&s_whist[0][0])[i] = 0u;
+    for (int i = tid; i < WARPS * kRsBins; i += kRsClThreads) (&s_whist[0][0])[i] = 0u;
     __syncthreads();
     K k[ITEMS];
     P v[ITEMS];
@@ -486,35 +487,41 @@ __global__ void __launch_bounds__(kRsThreads, 1) rs_cluster_kernel(K *keys, P *v
       else rank2[j >> 1] = r;
     }
     __syncthreads();
-    // thread d: the digit's count in this tile, its start in the staged tile
-    // per warp, and the count the peers read
+    // thread d < 256: the digit's count in this tile, its start in the
+    // staged tile per warp, and the count the peers read
     const int d = tid;
+    const bool dth = d < kRsBins;
     unsigned int cnt = 0;
+    if (dth) {
 #pragma unroll
-    for (int w = 0; w < kRsWarps; ++w) cnt += s_whist[w][d];
+      for (int w = 0; w < WARPS; ++w) cnt += s_whist[w][d];
+    }
     unsigned int tile_total;
-    const unsigned int tile_excl = block_exclusive_scan<kRsThreads>(cnt, OpSum<unsigned int>(), s_scan, tile_total);
-    {
+    const unsigned int tile_excl = block_exclusive_scan<kRsClThreads>(cnt, OpSum<unsigned int>(), s_scan, tile_total);
+    unsigned int real = 0;
+    if (dth) {
       unsigned int run = tile_excl;
 #pragma unroll
-      for (int w = 0; w < kRsWarps; ++w) {
+      for (int w = 0; w < WARPS; ++w) {
         const unsigned int c = s_whist[w][d];
         s_whist[w][d] = run;
         run += c;
       }
+      real = d == kRsBins - 1 ? cnt - (unsigned int)(kRsTile - count) : cnt;
+      s_cnt[d] = real;
     }
-    const unsigned int real = d == kRsBins - 1 ? cnt - (unsigned int)(kRsTile - count) : cnt;
-    s_cnt[d] = real;
     rs_cluster_sync();  // every tile's counts are visible in the cluster
     unsigned int before = 0, total = 0;
-    for (uint32_t q = 0; q < csize; ++q) {
-      const unsigned int c = q == me ? real : rs_peer_ld_u32(rs_peer_addr(&s_cnt[d], q));
-      total += c;
-      if (q < me) before += c;
+    if (dth) {
+      for (uint32_t q = 0; q < csize; ++q) {
+        const unsigned int c = q == me ? real : rs_peer_ld_u32(rs_peer_addr(&s_cnt[d], q));
+        total += c;
+        if (q < me) before += c;
+      }
     }
     unsigned int all;
-    const unsigned int start = block_exclusive_scan<kRsThreads>(total, OpSum<unsigned int>(), s_scan, all);
-    s_dst[d] = start + before - tile_excl;
+    const unsigned int start = block_exclusive_scan<kRsClThreads>(total, OpSum<unsigned int>(), s_scan, all);
+    if (dth) s_dst[d] = start + before - tile_excl;
     // stage in digit order in this pass's own buffer (every thread has read
     // its items: the scans above contain barriers)
 #pragma unroll
@@ -527,7 +534,7 @@ __global__ void __launch_bounds__(kRsThreads, 1) rs_cluster_kernel(K *keys, P *v
     __syncthreads();
     // staged position p goes to position g of the array: into the output
     // buffer of CTA g / tile, at g % tile
-    for (int p = tid; p < count; p += kRsThreads) {
+    for (int p = tid; p < count; p += kRsClThreads) {
       const K key = bk_(in)[p];
       const uint32_t g = s_dst[rs_digit(key, shift)] + (uint32_t)p;
       if (g < n) {  // always true when the counts are consistent
@@ -539,7 +546,7 @@ __global__ void __launch_bounds__(kRsThreads, 1) rs_cluster_kernel(K *keys, P *v
     rs_cluster_sync();  // every key of the pass has reached its tile
   }
   const int fin = rs_passes<K>() & 1;
-  for (int i = tid; i < count; i += kRsThreads) {
+  for (int i = tid; i < count; i += kRsClThreads) {
     keys[base + i] = bk_(fin)[i];
     if constexpr (has_payload<P>()) vals[base + i] = bv_(fin)[i];
   }
@@ -561,7 +568,7 @@ int rs_cluster_setup(int *max_ctas) {
     for (int c : {kRsClusterMax, 8}) {
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3((unsigned)c);
-      cfg.blockDim = dim3(kRsThreads);
+      cfg.blockDim = dim3(kRsClThreads);
       cfg.dynamicSmemBytes = smem;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -590,7 +597,7 @@ int rs_cluster_launch(K *keys, P *vals, uint64_t n, cudaStream_t stream) {
   const unsigned c = (unsigned)((n + kRsTile - 1) / kRsTile);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(c);
-  cfg.blockDim = dim3(kRsThreads);
+  cfg.blockDim = dim3(kRsClThreads);
   cfg.dynamicSmemBytes = rs_cluster_smem_bytes<K, P>();
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
