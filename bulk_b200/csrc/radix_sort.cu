@@ -405,10 +405,29 @@ __device__ __forceinline__ uint32_t rs_peer_addr(const void *local, uint32_t ran
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_addr(local)), "r"(rank));
   return r;
 }
+// (ordered by the cluster barriers around it, so no memory clobber: the
+// loads of one thread may all be in flight at once)
 __device__ __forceinline__ uint32_t rs_peer_ld_u32(uint32_t a) {
   uint32_t v;
-  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a));
   return v;
+}
+// Exclusive sum scan of v over threads 0-255 of the CTA (the digit threads;
+// the other warps do not take part), with the total; s_w holds 8 words.
+__device__ __forceinline__ unsigned int rs_scan_digits(unsigned int v, unsigned int *s_w, unsigned int &total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned int incl = warp_inclusive_scan(v, OpSum<unsigned int>(), lane);
+  if (lane == 31) s_w[warp] = incl;
+  named_barrier_sync(1, kRsBins);
+  unsigned int pre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kRsBins / 32; ++w) {
+    const unsigned int x = s_w[w];
+    tot += x;
+    if (w < warp) pre += x;
+  }
+  total = tot;
+  return pre + incl - v;
 }
 template <typename T>
 __device__ __forceinline__ void rs_peer_st(uint32_t a, T v) {
@@ -437,7 +456,7 @@ __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P 
   __shared__ unsigned int s_whist[WARPS][kRsBins];  // per-warp digit counters, then staging starts
   __shared__ unsigned int s_cnt[kRsBins];              // this tile's count of each digit (read by the peers)
   __shared__ unsigned int s_dst[kRsBins];  // output position of staged position 0 for digit d
-  __shared__ unsigned int s_scan[WARPS + 1];
+  __shared__ unsigned int s_scan[2 * (kRsBins / 32)];  // the two digit scans' warp totals
   auto bk_ = [&](int b) { return reinterpret_cast<K *>(rs_cl_smem + b * BB); };
   auto bv_ = [&](int b) { return reinterpret_cast<P *>(rs_cl_smem + b * BB + VOFF); };
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -487,19 +506,17 @@ __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P 
       else rank2[j >> 1] = r;
     }
     __syncthreads();
-    // thread d < 256: the digit's count in this tile, its start in the
-    // staged tile per warp, and the count the peers read
+    // thread d < 256 (warps 0-7, meeting on a named barrier): the digit's
+    // count in this tile, its start in the staged tile per warp, and the
+    // count the peers read; then its output offset from every tile's counts
     const int d = tid;
-    const bool dth = d < kRsBins;
-    unsigned int cnt = 0;
-    if (dth) {
+    unsigned int tile_excl = 0;
+    if (d < kRsBins) {
+      unsigned int cnt = 0;
 #pragma unroll
       for (int w = 0; w < WARPS; ++w) cnt += s_whist[w][d];
-    }
-    unsigned int tile_total;
-    const unsigned int tile_excl = block_exclusive_scan<kRsClThreads>(cnt, OpSum<unsigned int>(), s_scan, tile_total);
-    unsigned int real = 0;
-    if (dth) {
+      unsigned int tile_total;
+      tile_excl = rs_scan_digits(cnt, s_scan, tile_total);
       unsigned int run = tile_excl;
 #pragma unroll
       for (int w = 0; w < WARPS; ++w) {
@@ -507,23 +524,26 @@ __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P 
         s_whist[w][d] = run;
         run += c;
       }
-      real = d == kRsBins - 1 ? cnt - (unsigned int)(kRsTile - count) : cnt;
-      s_cnt[d] = real;
+      s_cnt[d] = d == kRsBins - 1 ? cnt - (unsigned int)(kRsTile - count) : cnt;
     }
-    rs_cluster_sync();  // every tile's counts are visible in the cluster
-    unsigned int before = 0, total = 0;
-    if (dth) {
-      for (uint32_t q = 0; q < csize; ++q) {
-        const unsigned int c = q == me ? real : rs_peer_ld_u32(rs_peer_addr(&s_cnt[d], q));
-        total += c;
-        if (q < me) before += c;
+    rs_cluster_sync();  // every tile's counts (and this tile's staging starts) are visible
+    if (d < kRsBins) {
+      unsigned int c[kRsClusterMax];
+#pragma unroll
+      for (int q = 0; q < kRsClusterMax; ++q)  // all loads in flight at once
+        c[q] = (uint32_t)q < csize ? rs_peer_ld_u32(rs_peer_addr(&s_cnt[d], (uint32_t)q)) : 0u;
+      unsigned int before = 0, total = 0;
+#pragma unroll
+      for (int q = 0; q < kRsClusterMax; ++q) {
+        total += c[q];
+        if ((uint32_t)q < me) before += c[q];
       }
+      unsigned int all;
+      const unsigned int start = rs_scan_digits(total, s_scan + kRsBins / 32, all);
+      s_dst[d] = start + before - tile_excl;
     }
-    unsigned int all;
-    const unsigned int start = block_exclusive_scan<kRsClThreads>(total, OpSum<unsigned int>(), s_scan, all);
-    if (dth) s_dst[d] = start + before - tile_excl;
     // stage in digit order in this pass's own buffer (every thread has read
-    // its items: the scans above contain barriers)
+    // its items: the cluster barrier above came after them)
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
       const int dj = digit_of(j);
