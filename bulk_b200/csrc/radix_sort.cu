@@ -27,6 +27,10 @@
 // A batch lays its arrays' count regions one after another, so the one scan
 // serves all of them: an array's positions are the scanned values minus the
 // number of elements of the arrays before it.
+//
+// A single array of up to 16 tiles is sorted instead by one launch of one
+// thread-block cluster that keeps the array in its CTAs' shared memory for
+// every pass (rs_cluster_kernel below).
 #include <type_traits>
 
 #include "bk_common.cuh"
@@ -405,8 +409,9 @@ __device__ __forceinline__ uint32_t rs_peer_addr(const void *local, uint32_t ran
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_addr(local)), "r"(rank));
   return r;
 }
-// (ordered by the cluster barriers around it, so no memory clobber: the
-// loads of one thread may all be in flight at once)
+// Load from another CTA's shared memory.  The cluster barriers around its
+// uses order it, so it has no memory clobber and one thread's loads may all
+// be in flight at once.
 __device__ __forceinline__ uint32_t rs_peer_ld_u32(uint32_t a) {
   uint32_t v;
   asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a));
@@ -429,6 +434,8 @@ __device__ __forceinline__ unsigned int rs_scan_digits(unsigned int v, unsigned 
   total = tot;
   return pre + incl - v;
 }
+// Store to another CTA's shared memory (seen there after the next cluster
+// barrier).
 template <typename T>
 __device__ __forceinline__ void rs_peer_st(uint32_t a, T v) {
   if constexpr (sizeof(T) == 4) {
