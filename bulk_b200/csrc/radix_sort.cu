@@ -474,12 +474,12 @@ __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P 
     bk_(0)[i] = keys[base + i];
     if constexpr (has_payload<P>()) bv_(0)[i] = vals[base + i];
   }
+  for (int i = tid; i < WARPS * kRsBins; i += kRsClThreads) (&s_whist[0][0])[i] = 0u;
+  __syncthreads();
   const unsigned int lt = (1u << lane) - 1u;
   for (int pass = 0; pass < rs_passes<K>(); ++pass) {
     const int in = pass & 1, out = in ^ 1;
     const int shift = 8 * pass;
-    for (int i = tid; i < WARPS * kRsBins; i += kRsClThreads) (&s_whist[0][0])[i] = 0u;
-    __syncthreads();
     K k[ITEMS];
     P v[ITEMS];
     auto elem = [&](int j) { return warp * 32 * ITEMS + j * 32 + lane; };
@@ -559,6 +559,10 @@ __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P 
       if constexpr (has_payload<P>()) bv_(in)[pos] = v[j];
     }
     __syncthreads();
+    // the counters start the next pass at zero (their last reader was the
+    // staging above; the cluster barrier below orders this before the next
+    // pass's ranking)
+    for (int i = tid; i < WARPS * kRsBins; i += kRsClThreads) (&s_whist[0][0])[i] = 0u;
     // staged position p goes to position g of the array: into the output
     // buffer of CTA g / tile, at g % tile
     for (int p = tid; p < count; p += kRsClThreads) {

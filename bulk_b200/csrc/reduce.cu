@@ -7,7 +7,7 @@
 //
 // Here one launch does it all: a grid of (SMs x CTAs-per-SM) CTAs streams the
 // input with 16-byte non-coherent loads (UNROLL independent loads in flight
-// per thread), each thread keeps UNROLL*V independent accumulators, the CTA
+// per thread), each thread keeps 4*V independent accumulators, the CTA
 // folds them with warp shuffles, writes one partial to the workspace, and the
 // last CTA to finish (atomic counter) folds the partials in index order and
 // writes init (+) total to d_out.  The partition of the input depends only on
@@ -36,17 +36,18 @@ size_t reduce_ws_bytes(int sm_count) {
 }
 
 template <typename T, typename Op>
-__global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const T *__restrict__ in, uint64_t head, uint64_t nvec,
+__global__ void __launch_bounds__(kReduceThreads, 4) reduce_kernel(const T *__restrict__ in, uint64_t head, uint64_t nvec,
                                                                  uint64_t tail, T init, T *__restrict__ out,
                                                                  T *__restrict__ partials, WsHeader *hdr) {
   constexpr int V = ReduceLayout<T>::V;
   constexpr int U = kReduceUnroll;
+  constexpr int A = 4;  // accumulator vectors: load u folds into acc[u % A]
   Op op;
-  T acc[U][V];
+  T acc[A][V];
 #pragma unroll
-  for (int u = 0; u < U; ++u)
+  for (int a = 0; a < A; ++a)
 #pragma unroll
-    for (int j = 0; j < V; ++j) acc[u][j] = Op::identity();
+    for (int j = 0; j < V; ++j) acc[a][j] = Op::identity();
 
   const int tid = threadIdx.x;
   const uint4 *vin = reinterpret_cast<const uint4 *>(in + head);
@@ -63,15 +64,26 @@ __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const T *__restr
       T e[V];
       memcpy(e, &r[u], 16);
 #pragma unroll
-      for (int j = 0; j < V; ++j) acc[u][j] = op(acc[u][j], e[j]);
+      for (int j = 0; j < V; ++j) acc[u % A][j] = op(acc[u % A][j], e[j]);
     }
   }
-  for (; v < nvec; v += stride) {
-    uint4 r = ld_stream_v4(vin + v);
-    T e[V];
-    memcpy(e, &r, 16);
+  // Fewer than U strides left: one more batch with each load predicated, so
+  // the last loads are in flight together instead of one DRAM round trip
+  // apiece.
+  {
+    uint4 r[U];
 #pragma unroll
-    for (int j = 0; j < V; ++j) acc[0][j] = op(acc[0][j], e[j]);
+    for (int u = 0; u < U - 1; ++u)
+      if (v + u * stride < nvec) r[u] = ld_stream_v4(vin + v + u * stride);
+#pragma unroll
+    for (int u = 0; u < U - 1; ++u) {
+      if (v + u * stride < nvec) {
+        T e[V];
+        memcpy(e, &r[u], 16);
+#pragma unroll
+        for (int j = 0; j < V; ++j) acc[u % A][j] = op(acc[u % A][j], e[j]);
+      }
+    }
   }
   // Unaligned head and ragged tail (fewer than V elements each): CTA 0.
   if (blockIdx.x == 0) {
@@ -81,9 +93,9 @@ __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const T *__restr
 
   // Fold the thread's accumulators pairwise (fixed order).
 #pragma unroll
-  for (int w = 1; w < U * V; w <<= 1) {
+  for (int w = 1; w < A * V; w <<= 1) {
 #pragma unroll
-    for (int i = 0; i + w < U * V; i += 2 * w) {
+    for (int i = 0; i + w < A * V; i += 2 * w) {
       acc[i / V][i % V] = op(acc[i / V][i % V], acc[(i + w) / V][(i + w) % V]);
     }
   }
