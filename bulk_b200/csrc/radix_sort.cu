@@ -28,7 +28,7 @@
 // serves all of them: an array's positions are the scanned values minus the
 // number of elements of the arrays before it.
 //
-// A single array of up to 16 tiles is sorted instead by one launch of one
+// A single array of up to 131,072 keys is sorted instead by one launch of one
 // thread-block cluster whose CTAs exchange their digit counts through
 // distributed shared memory (rs_cluster_kernel below).
 #include <type_traits>
@@ -376,8 +376,8 @@ __global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downswe
 }
 
 // ---------------------------------------------------------------------------
-// Small arrays (up to 16 tiles): every pass in one launch of one thread-block
-// cluster, one CTA per tile.  The CTAs exchange their digit counts through
+// Small arrays (up to 16 tiles of 4096 or 8192 keys): every pass in one launch
+// of one thread-block cluster, one CTA per tile.  The CTAs exchange their digit counts through
 // distributed shared memory (each reads every other CTA's 256 counts across
 // the cluster) instead of a count scan in global memory, and a cluster barrier
 // takes the place of each kernel boundary: two barriers a pass replace the
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(TH, rs_down_min_blocks<TH, K, P>()) rs_downswe
 // sizes (storing each key straight into the owning CTA's shared memory was
 // measured slower: 42.9 against 32.8 us for 2^16 u32/u32 keys on a B200).
 constexpr int kRsClusterMax = 16;  // CTAs (non-portable above 8)
-constexpr int kRsClThreads = 1024;  // four items a thread: short ranking chains, 32 warps an SM
+constexpr int kRsClThreads = 1024;  // four or eight items a thread: short ranking chains, 32 warps an SM
 
 __device__ __forceinline__ uint32_t rs_cluster_rank() {
   uint32_t r;
@@ -434,25 +434,26 @@ __device__ __forceinline__ unsigned int rs_scan_digits(unsigned int v, unsigned 
   total = tot;
   return pre + incl - v;
 }
-// Shared memory of a cluster-sort CTA: one tile of keys and payloads.
-template <typename K, typename P>
+// Shared memory of a cluster-sort CTA of ITEMS items a thread: one tile
+// (1024 * ITEMS keys and payloads).
+template <typename K, typename P, int ITEMS>
 constexpr size_t rs_cluster_smem_bytes() {
-  return align_up(sizeof(K) * kRsTile, 16) + (size_t)payload_bytes<P>() * kRsTile;
+  return align_up(sizeof(K) * kRsClThreads * ITEMS, 16) + (size_t)payload_bytes<P>() * kRsClThreads * ITEMS;
 }
 
 // The cluster sort: CTA r of the cluster owns tile r.  Each pass reads the
 // tile from the pass's input (the array on even passes, the workspace
 // temporaries on odd ones; all L2-resident at these sizes), ranks its keys as
-// the scatter above does (four items a thread), exchanges its 256 digit
+// the scatter above does (ITEMS items a thread), exchanges its 256 digit
 // counts with the other CTAs through distributed shared memory, stages the
 // tile in digit order and writes each digit's run to the pass's output.  The
 // cluster barrier after the writes (release / acquire at cluster scope) makes
 // them visible to the CTA that reads that tile next.  Even passes end in the
 // array, so the last one leaves the result in place.
-template <typename K, typename P>
+template <typename K, typename P, int ITEMS>
 __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P *vals, K *tk, P *tv, uint32_t n) {
-  constexpr int ITEMS = kRsTile / kRsClThreads, WARPS = kRsClThreads / 32;
-  constexpr size_t VOFF = align_up(sizeof(K) * kRsTile, 16);
+  constexpr int WARPS = kRsClThreads / 32, TILE = kRsClThreads * ITEMS;
+  constexpr size_t VOFF = align_up(sizeof(K) * TILE, 16);
   extern __shared__ __align__(16) unsigned char rs_cl_smem[];
   K *sk = reinterpret_cast<K *>(rs_cl_smem);  // the tile in digit order
   P *sv = reinterpret_cast<P *>(rs_cl_smem + VOFF);
@@ -462,8 +463,8 @@ __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P 
   __shared__ unsigned int s_scan[2 * (kRsBins / 32)];  // the two digit scans' warp totals
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t me = rs_cluster_rank(), csize = rs_cluster_size();
-  const uint32_t base = me * (uint32_t)kRsTile;
-  const int count = (int)((n - base) < (uint32_t)kRsTile ? (n - base) : (uint32_t)kRsTile);
+  const uint32_t base = me * (uint32_t)TILE;
+  const int count = (int)((n - base) < (uint32_t)TILE ? (n - base) : (uint32_t)TILE);
   for (int i = tid; i < WARPS * kRsBins; i += kRsClThreads) (&s_whist[0][0])[i] = 0u;
   __syncthreads();
   const unsigned int lt = (1u << lane) - 1u;
@@ -519,7 +520,7 @@ __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P 
         s_whist[w][d] = run;
         run += c;
       }
-      s_cnt[d] = d == kRsBins - 1 ? cnt - (unsigned int)(kRsTile - count) : cnt;
+      s_cnt[d] = d == kRsBins - 1 ? cnt - (unsigned int)(TILE - count) : cnt;
     }
     rs_cluster_sync();
     if (d < kRsBins) {
@@ -559,13 +560,13 @@ __global__ void __launch_bounds__(kRsClThreads, 1) rs_cluster_kernel(K *keys, P 
 }
 
 // Once per device: the largest cluster (16 or 8 CTAs, 0 for none) that the
-// cluster sort can be launched with.
-template <typename K, typename P>
+// cluster sort can be launched with, for tiles of 1024 * ITEMS keys.
+template <typename K, typename P, int ITEMS>
 int rs_cluster_setup(int *max_ctas) {
   struct Site {};
   return host::once_per_device<Site>(max_ctas, [](int *mx) -> int {
-    auto kern = rs_cluster_kernel<K, P>;
-    constexpr size_t smem = rs_cluster_smem_bytes<K, P>();
+    auto kern = rs_cluster_kernel<K, P, ITEMS>;
+    constexpr size_t smem = rs_cluster_smem_bytes<K, P, ITEMS>();
     int st;
     if ((st = host::set_smem_attrs(kern, smem)) != BK_OK) return st;
     *mx = 0;
@@ -597,15 +598,16 @@ int rs_cluster_setup(int *max_ctas) {
   });
 }
 
-// The cluster sort of n elements (n <= kRsTile * max_ctas), one launch;
+// The cluster sort of n elements (n <= 1024 * ITEMS * max_ctas), one launch;
 // tk / tv are the workspace temporaries of n elements.
-template <typename K, typename P>
+template <typename K, typename P, int ITEMS>
 int rs_cluster_launch(K *keys, P *vals, K *tk, P *tv, uint64_t n, cudaStream_t stream) {
-  const unsigned c = (unsigned)((n + kRsTile - 1) / kRsTile);
+  constexpr uint64_t TILE = (uint64_t)kRsClThreads * ITEMS;
+  const unsigned c = (unsigned)((n + TILE - 1) / TILE);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(c);
   cfg.blockDim = dim3(kRsClThreads);
-  cfg.dynamicSmemBytes = rs_cluster_smem_bytes<K, P>();
+  cfg.dynamicSmemBytes = rs_cluster_smem_bytes<K, P, ITEMS>();
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -614,7 +616,7 @@ int rs_cluster_launch(K *keys, P *vals, K *tk, P *tv, uint64_t n, cudaStream_t s
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return host::from_cuda(cudaLaunchKernelEx(&cfg, rs_cluster_kernel<K, P>, keys, vals, tk, tv, (uint32_t)n));
+  return host::from_cuda(cudaLaunchKernelEx(&cfg, rs_cluster_kernel<K, P, ITEMS>, keys, vals, tk, tv, (uint32_t)n));
 }
 
 template <typename K, typename P>
@@ -712,14 +714,16 @@ int radix_sort_launch(K *keys, P *vals, uint64_t n, void *d_ws, size_t ws_bytes,
   if (n >= kRsMaxN) return BK_ERR_TOO_LARGE;  // the caller sorts these by merging
   const RsLayout<K, P> L(&n, 1);
   if ((st = host::check_ws(d_ws, ws_bytes, L.total)) != BK_OK) return st;
-  int cl_max = 0;
-  if ((st = rs_cluster_setup<K, P>(&cl_max)) != BK_OK) return st;
   char *ws = reinterpret_cast<char *>(d_ws);
   K *tk = reinterpret_cast<K *>(ws + L.tmp);
   P *tv = reinterpret_cast<P *>(ws + L.tmp + align_up(n * sizeof(K), 256));
-  if (n <= (uint64_t)kRsTile * (uint64_t)cl_max) {
-    return rs_cluster_launch<K, P>(keys, vals, tk, tv, n, stream);
-  }
+  // one cluster launch: four items a thread up to 16 tiles of 4096 keys (more
+  // CTAs, a shorter pass), eight up to 16 tiles of 8192
+  int cl4 = 0, cl8 = 0;
+  if ((st = rs_cluster_setup<K, P, 4>(&cl4)) != BK_OK) return st;
+  if (n <= (uint64_t)kRsClThreads * 4 * (uint64_t)cl4) return rs_cluster_launch<K, P, 4>(keys, vals, tk, tv, n, stream);
+  if ((st = rs_cluster_setup<K, P, 8>(&cl8)) != BK_OK) return st;
+  if (n <= (uint64_t)kRsClThreads * 8 * (uint64_t)cl8) return rs_cluster_launch<K, P, 8>(keys, vals, tk, tv, n, stream);
   return radix_sort_run<K, P>(RsOne<K, P>{keys, vals, tk, tv, n, (uint32_t)L.tiles}, L, ws, stream);
 }
 

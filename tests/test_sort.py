@@ -42,9 +42,10 @@ def _keys(tag, n, seed, coarse):
 @pytest.mark.parametrize("tag", KEYS)
 @pytest.mark.parametrize("payload", [None, np.uint32, np.uint64])
 def test_edge_sizes(cuda, tag, payload):
-    # 8193-65536 elements: one cluster launch (one CTA per 4096-key tile, up
-    # to 16); above: the global-memory radix passes
-    sizes = [0, 1, 2, 3, 17, 1023, 4096, 8191, 8192, 8193, 16385, 3 * 8192 + 5, 32769, 65536, 65537, 100003]
+    # 8193-131072 elements: one cluster launch (up to 16 CTAs of 4096-key,
+    # then of 8192-key tiles); above: the global-memory radix passes
+    sizes = [0, 1, 2, 3, 17, 1023, 4096, 8191, 8192, 8193, 16385, 3 * 8192 + 5, 32769, 65536, 65537, 100003,
+             131072, 131075, 300007]
     for i, n in enumerate(sizes):
         for coarse in (False, True):
             keys = _keys(tag, n, 300 + i, coarse)
