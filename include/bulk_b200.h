@@ -221,9 +221,10 @@ BK_API int bk_merge_by_key_f64_u64(const double *a_keys, const uint64_t *a_vals,
  * 152-166, stable_merge_sort.hpp:125-206, then merge-path passes).  The
  * stable order is unique, so the result is the reference's whichever way it
  * is computed: one block sort for an array of one tile (8192 4-byte / 4096
- * 8-byte keys), a stable LSD radix sort below 2^30 elements, block sort and
- * merge-path passes from 2^30 on.  Keys must not be NaN.  bk_sort_keys_*
- * sorts keys alone. */
+ * 8-byte keys), a stable LSD radix sort below 2^30 elements (up to 131,072
+ * keys as one launch of one thread-block cluster, above that as passes of
+ * three launches each), block sort and merge-path passes from 2^30 on.  Keys
+ * must not be NaN.  bk_sort_keys_* sorts keys alone. */
 BK_API int bk_sort_keys_i32(int32_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_sort_keys_u32(uint32_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
 BK_API int bk_sort_keys_i64(int64_t *keys, uint64_t n, void *d_ws, size_t ws_bytes, bk_stream_t stream);
